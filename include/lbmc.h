@@ -1,0 +1,223 @@
+/*
+ * lbmc.h — C ABI of the B200 lattice Boltzmann time-step engine.
+ *
+ * This is the drop-in boundary for LBM-C's time-step path.  Each entry point
+ * replaces one piece of the reference's host code (paths are relative to the
+ * LBM-C project root):
+ *
+ *   lbmc_init      setup()            LBM-C/index.cu:157-186 and the
+ *                  ModelBuilder       LBM-C/model_builder.cu:63-248
+ *                  (constant upload, SoA allocation, field upload, Init 0)
+ *   lbmc_iterate   iterate(int t)     LBM-C/index.cu:284-313 (one launch of
+ *                  iterate_kernel, LBM-C/solver.cu:10-136, per time step)
+ *   lbmc_fetch     output_macros      LBM-C/index.cu:196-216,
+ *                  screen_mess        LBM-C/index.cu:412-432,
+ *                  current_RMS        LBM-C/index.cu:338-373 (KE sum)
+ *   lbmc_destroy   (none: the reference never frees its device state)
+ *
+ * Conventions kept from the reference:
+ *   - node order ixd = x + y*Lx + z*Lx*Ly (LBM-C/solver.cu:23);
+ *   - lattice velocity order, weights and opposites of LBM-C/macros.cu:19-53
+ *     (D2Q9) and :71-119 (D3Q15);
+ *   - ColType codes BGK=0, NTPOR=1, MRT=2, MRTPOR=3
+ *     (LBM-C/infile_reader.cu:118-144);
+ *   - MacroBC codes 1..15 (LBM-C/boundary_conditions/macro_bc.cu:12-17) and
+ *     MicroBC codes 1..8 (D2Q9) / 1..12 (D3Q15)
+ *     (LBM-C/boundary_conditions/micro_bc.cuh:7-15), used verbatim;
+ *   - Porosity B >= 1 selects full-way bounceback (LBM-C/solver.cu:67-72);
+ *   - the prescribed rho/u fields are also where stored macros are written
+ *     (LBM-C/solver.cu:126-134 writes Domain.u/rho, which macro_bc.cu reads).
+ *
+ * Differences: every call returns an lbmc_status and never exits the process
+ * (the reference calls exit(-1), LBM-C/cuda_util.cu:14-27); handles are
+ * independent (the reference keeps one instance in file-scope globals,
+ * LBM-C/index.cu:40-59); the step counter lives in the handle.
+ *
+ * Thread safety: calls on one handle must not overlap; separate handles may
+ * be used from separate threads.
+ */
+#ifndef LBMC_H
+#define LBMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBMC_API_VERSION 1
+#define LBMC_MAX_Q 15
+
+typedef enum lbmc_status {
+  LBMC_OK = 0,
+  LBMC_ERR_INVALID_ARG = 1,  /* bad pointer, size, code or parameter */
+  LBMC_ERR_UNSUPPORTED = 2,  /* valid input this build does not handle */
+  LBMC_ERR_CUDA = 3,         /* CUDA runtime error; see lbmc_last_error() */
+  LBMC_ERR_ALLOC = 4,        /* device or host allocation failed */
+  LBMC_ERR_NAN = 5,          /* non-finite density/velocity detected */
+  LBMC_ERR_TIMEOUT = 6,      /* a bounded device-side wait expired */
+  LBMC_ERR_IO = 7,           /* file could not be read or parsed */
+  LBMC_ERR_BUFFER_SIZE = 8,  /* destination buffer too small */
+  LBMC_ERR_NO_DEVICE = 9     /* no usable CUDA device */
+} lbmc_status;
+
+typedef enum lbmc_lattice { LBMC_D2Q9 = 0, LBMC_D3Q15 = 1 } lbmc_lattice;
+
+/* Population storage in HBM.  All formats hold f_i - w_i (deviation from the
+ * rest-state weight); arithmetic is FP32, or FP64 for LBMC_F64. */
+typedef enum lbmc_storage {
+  LBMC_F32 = 0,
+  LBMC_F16 = 1,
+  LBMC_BF16 = 2,
+  LBMC_F64 = 3
+} lbmc_storage;
+
+/* ColType codes of LBM-C/infile_reader.cu:118-144. */
+typedef enum lbmc_collision {
+  LBMC_BGK = 0,
+  LBMC_NTPOR = 1,
+  LBMC_MRT = 2,
+  LBMC_MRTPOR = 3
+} lbmc_collision;
+
+typedef enum lbmc_init_type {
+  LBMC_INIT_STATIC = 0,      /* f = w_i (rho = 1, u = 0): the reference's Init 0 */
+  LBMC_INIT_EQUILIBRIUM = 1, /* f = f_eq(rho, u) from lbmc_domain.rho / .u */
+  LBMC_INIT_F = 2            /* f from lbmc_domain.f (restart / checkpoint) */
+} lbmc_init_type;
+
+typedef enum lbmc_streaming {
+  LBMC_STREAM_SHIFT = 0, /* in place, population i of node x at (x - t e_i) mod L */
+  LBMC_STREAM_AA = 1     /* in place, AA pattern (even/odd step index maps) */
+} lbmc_streaming;
+
+/* Reproduce documented reference defects exactly ("as-is" behaviour). */
+#define LBMC_COMPAT_D3Q15_MINV_ZERO (1u << 0) /* macros.cu:97-115: D3Q15 MRT relaxes nothing */
+#define LBMC_COMPAT_MEQ_INT_DIV (1u << 1)     /* collision.cu:492-496: (-7/3) evaluates to -2 */
+#define LBMC_COMPAT_ZH_Z_UX (1u << 2)         /* d3q15_zh_defs.cu:87-91: -z Zou-He uses u[0] */
+#define LBMC_COMPAT_MRTPOR_INPLACE (1u << 3)  /* collision.cu:340,416: blend reads updated f[opp] */
+#define LBMC_COMPAT_REFERENCE_AS_IS                                              \
+  (LBMC_COMPAT_D3Q15_MINV_ZERO | LBMC_COMPAT_MEQ_INT_DIV | LBMC_COMPAT_ZH_Z_UX | \
+   LBMC_COMPAT_MRTPOR_INPLACE)
+
+/* Mirrors the fields of DomainConstant (LBM-C/data_types.cuh:23-43) that the
+ * input file sets, plus the engine's own choices. */
+typedef struct lbmc_config {
+  int lattice;          /* lbmc_lattice */
+  int length[3];        /* Lx, Ly, Lz; Lz must be 1 for D2Q9 */
+  double tau;           /* Tau */
+  double tau_mrt[LBMC_MAX_Q]; /* TauMRT: MRT relaxation rates, first Q used */
+  double c_smag;        /* C_smag; > 0 enables Smagorinsky (BGK family only) */
+  int collision_type;   /* ColType, lbmc_collision */
+  int forcing;          /* Force: Guo body force from lbmc_domain.force */
+  int macro_bc;         /* MacroBC: per-node prescribed rho/u codes */
+  int micro_bc;         /* MicroBC: per-node Zou-He / stress-free codes */
+  int init_type;        /* Init, lbmc_init_type */
+  double tolerance;     /* Tolerance (used by drivers, not by the step) */
+  int h, dt;            /* DeltaX, DeltaT (carried, unused by the step, as in the reference) */
+  int storage;          /* lbmc_storage */
+  int streaming;        /* lbmc_streaming */
+  unsigned compat;      /* LBMC_COMPAT_* bits */
+  double storage_scale; /* stored value = (f - w) * scale; 0 selects the default */
+  int device;           /* CUDA device ordinal */
+  int block_size;       /* threads per block of the step kernel; 0 = tuned default */
+  int reserved[6];
+} lbmc_config;
+
+/* Host arrays in ixd order; the caller keeps ownership, lbmc_init copies.
+ * Mirrors Domain (LBM-C/data_types.cuh:13-21) plus the initial state. */
+typedef struct lbmc_domain {
+  const double *geometry; /* N: Porosity B in [0,1]; B >= 1 solid; NULL = all fluid */
+  const double *force[3]; /* N each when forcing; NULL component = 0 */
+  const int *macro_bc;    /* N MacroBC codes (0 = none) when macro_bc */
+  const int *micro_bc;    /* N MicroBC codes (0 = none) when micro_bc */
+  const double *u[3];     /* N each: prescribed velocity (macro BC) / initial velocity */
+  const double *rho;      /* N: prescribed density (macro BC) / initial density */
+  const double *f;        /* Q*N natural-layout populations for LBMC_INIT_F */
+} lbmc_domain;
+
+typedef struct lbmc_handle lbmc_handle;
+
+/* lbmc_iterate flags. */
+#define LBMC_STORE_MACROS (1u << 0) /* write rho/u on the last step of the call */
+#define LBMC_REDUCE_DIAG (1u << 1)  /* FP64 mass/momentum/KE sums on the last step */
+#define LBMC_SYNC (1u << 2)         /* wait for completion and report errors/NaN */
+
+/* lbmc_fetch fields. */
+typedef enum lbmc_field {
+  LBMC_FIELD_RHO = 0, /* N doubles: stored density */
+  LBMC_FIELD_U_X = 1, /* N doubles: stored velocity components */
+  LBMC_FIELD_U_Y = 2,
+  LBMC_FIELD_U_Z = 3,
+  LBMC_FIELD_F = 4,   /* Q*N doubles: populations f_i in natural layout */
+  LBMC_FIELD_DIAG = 5 /* one lbmc_diag */
+} lbmc_field;
+
+typedef struct lbmc_diag {
+  double mass;           /* sum of rho over all nodes (solids hold rho = 0) */
+  double momentum[3];    /* sum of rho*u */
+  double kinetic_energy; /* sum of 0.5*rho*|u|^2, current_RMS (index.cu:338-373) */
+  long long step;        /* completed steps when the sums were taken */
+  int nonfinite;         /* 1 if any rho or u was NaN/Inf */
+  int valid;             /* 1 once a LBMC_REDUCE_DIAG step has run */
+} lbmc_diag;
+
+/* Fills cfg with the reference's defaults for a lattice (c_smag = 0 as in
+ * InfileReader::initialise, LBM-C/infile_reader.cu:20-23). */
+lbmc_status lbmc_config_default(lbmc_config *cfg, int lattice);
+
+/* Replaces setup() (LBM-C/index.cu:157-186) and ModelBuilder
+ * (LBM-C/model_builder.cu:257-278). */
+lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
+                      lbmc_handle **out);
+
+/* Replaces nsteps calls of iterate(t) (LBM-C/index.cu:284-313).  The step
+ * counter t continues across calls.  Without LBMC_SYNC the call only
+ * enqueues work on the handle's stream. */
+lbmc_status lbmc_iterate(lbmc_handle *h, int nsteps, unsigned flags);
+
+/* Replaces the device-to-host copies of output_macros / screen_mess /
+ * compute_residual (LBM-C/index.cu:196-216, 412-432, 387-409).  Blocks until
+ * the handle's stream is idle. */
+lbmc_status lbmc_fetch(lbmc_handle *h, int field, void *dst, size_t bytes);
+
+lbmc_status lbmc_destroy(lbmc_handle *h);
+
+/* Completed time steps (the t the next step will use). */
+lbmc_status lbmc_get_step(lbmc_handle *h, long long *step);
+
+/* Runs the handle's work on a caller stream (a cudaStream_t); NULL = the
+ * handle's own stream. */
+lbmc_status lbmc_set_stream(lbmc_handle *h, void *cuda_stream);
+
+lbmc_status lbmc_synchronize(lbmc_handle *h);
+
+const char *lbmc_status_string(lbmc_status s);
+
+/* Host-only helpers (no GPU needed). */
+
+/* Checks a configuration and domain the way lbmc_init does, without touching
+ * the GPU (the reference validates nothing and crashes on bad codes, e.g. the
+ * NULL D2Q9 MicroBC entries 3 and 4 of micro_bc.cuh:7-8). */
+lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *dom);
+
+/* The per-node class bytes and class table lbmc_init would upload: class 0
+ * plain fluid, 1 solid (Porosity >= 1), >= 2 an index into table, whose
+ * entries pack MacroBC (bits 0-3), MicroBC (bits 4-7) and a partial-solid
+ * bit (bit 8).  cls_out holds N bytes, table_out 256 entries. */
+lbmc_status lbmc_classify(const lbmc_config *cfg, const lbmc_domain *dom, uint8_t *cls_out,
+                          uint16_t *table_out, int *nclasses);
+
+/* Lattice tables as the kernels use them: e[DIM*Q] (row per axis), w[Q],
+ * opp[Q], M[Q*Q] (LBM-C/macros.cu:19-53, 71-119). */
+lbmc_status lbmc_lattice_tables(int lattice, int *e, double *w, int *opp, int *m);
+
+/* Message of the last error on the calling thread ("" if none). */
+const char *lbmc_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBMC_H */

@@ -1,0 +1,657 @@
+// C-ABI engine: lbmc_init / lbmc_iterate / lbmc_fetch / lbmc_destroy.
+//
+// Host side of the drop-in boundary for LBM-C's time-step path.  lbmc_init
+// plays the role of setup() + ModelBuilder (LBM-C/index.cu:157-186,
+// LBM-C/model_builder.cu:63-248): it validates the configuration, packs the
+// per-node inputs (Porosity, MacroBC, MicroBC) into one class byte per node
+// plus a class table, uploads the fields and sets the initial populations.
+// lbmc_iterate replaces iterate(t) (LBM-C/index.cu:284-313) and enqueues one
+// fused step kernel per time step on the handle's stream; lbmc_fetch replaces
+// the device-to-host copies of output_macros / screen_mess /
+// compute_residual (LBM-C/index.cu:196-216, 387-439).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/lbmc.h"
+#include "engine_internal.h"
+#include "kernels.cuh"
+#include "lattice.cuh"
+
+using namespace lbmc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+lbmc_status fail(lbmc_status s, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+lbmc_status cuda_fail(cudaError_t e, const char *what) {
+  return fail(e == cudaErrorMemoryAllocation ? LBMC_ERR_ALLOC : LBMC_ERR_CUDA, "%s: %s", what,
+              cudaGetErrorString(e));
+}
+
+#define CK(call, what)                          \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+int lattice_q(int lattice) { return lattice == LBMC_D2Q9 ? 9 : 15; }
+int lattice_dim(int lattice) { return lattice == LBMC_D2Q9 ? 2 : 3; }
+
+double lattice_w(int lattice, int i) {
+  return lattice == LBMC_D2Q9 ? (double)D2Q9::wn(i) / D2Q9::wd : (double)D3Q15::wn(i) / D3Q15::wd;
+}
+int lattice_e(int lattice, int d, int i) {
+  return lattice == LBMC_D2Q9 ? D2Q9::e(d, i) : D3Q15::e(d, i);
+}
+
+const LatticeStorageOps *select_ops(int lattice, int storage) {
+  if (lattice == LBMC_D2Q9) {
+    switch (storage) {
+      case LBMC_F32: return ops_d2q9_f32();
+      case LBMC_F16: return ops_d2q9_f16();
+      case LBMC_BF16: return ops_d2q9_bf16();
+      case LBMC_F64: return ops_d2q9_f64();
+    }
+  } else {
+    switch (storage) {
+      case LBMC_F32: return ops_d3q15_f32();
+      case LBMC_F16: return ops_d3q15_f16();
+      case LBMC_BF16: return ops_d3q15_bf16();
+      case LBMC_F64: return ops_d3q15_f64();
+    }
+  }
+  return nullptr;
+}
+
+bool is_sf_code(int lattice, int code) {
+  return lattice == LBMC_D2Q9 ? (code >= 5 && code <= 8) : (code >= 7 && code <= 12);
+}
+
+// Host-side packing of the per-node inputs.
+struct HostClasses {
+  std::vector<uint8_t> cls;
+  uint16_t table[256];
+  int nclasses = 2;
+  std::vector<int> sf_nodes;
+  std::vector<uint8_t> sf_face;
+  bool any_partial = false;
+};
+
+}  // namespace
+
+struct lbmc_handle {
+  lbmc_config cfg;
+  DeviceState ds;
+  const LatticeStorageOps *ops = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  long long step = 0;
+  long long nblocks = 0;
+  double *diag_out = nullptr;  // DIAG_VALUES doubles
+  long long diag_step = -1;
+  std::vector<void *> allocations;
+};
+
+// ------------------------------------------------------------ validation
+
+extern "C" lbmc_status lbmc_config_default(lbmc_config *cfg, int lattice) {
+  if (!cfg) return fail(LBMC_ERR_INVALID_ARG, "lbmc_config_default: cfg is NULL");
+  if (lattice != LBMC_D2Q9 && lattice != LBMC_D3Q15)
+    return fail(LBMC_ERR_INVALID_ARG, "lbmc_config_default: unknown lattice %d", lattice);
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->lattice = lattice;
+  cfg->length[0] = cfg->length[1] = 1;
+  cfg->length[2] = 1;
+  cfg->tau = 1.0;
+  cfg->c_smag = 0.0;
+  cfg->collision_type = LBMC_BGK;
+  cfg->init_type = LBMC_INIT_STATIC;
+  cfg->storage = LBMC_F32;
+  cfg->streaming = LBMC_STREAM_SHIFT;
+  cfg->compat = 0;
+  cfg->storage_scale = 0.0;
+  return LBMC_OK;
+}
+
+static double default_scale(int storage) { return storage == LBMC_F16 ? 1024.0 : 1.0; }
+
+// Checks a configuration and domain without touching the GPU.
+extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *dom) {
+  if (!cfg) return fail(LBMC_ERR_INVALID_ARG, "config is NULL");
+  if (cfg->lattice != LBMC_D2Q9 && cfg->lattice != LBMC_D3Q15)
+    return fail(LBMC_ERR_INVALID_ARG, "unknown lattice %d", cfg->lattice);
+  const int dim = lattice_dim(cfg->lattice);
+  long long n = 1;
+  for (int d = 0; d < 3; d++) {
+    if (cfg->length[d] < 1) return fail(LBMC_ERR_INVALID_ARG, "length[%d] = %d must be >= 1", d, cfg->length[d]);
+    if (d < dim) n *= cfg->length[d];
+  }
+  if (dim == 2 && cfg->length[2] != 1)
+    return fail(LBMC_ERR_INVALID_ARG, "D2Q9 needs length[2] == 1 (got %d)", cfg->length[2]);
+  if (n > 0x7FFFFFFFLL - 1024)
+    return fail(LBMC_ERR_UNSUPPORTED, "%lld nodes exceed the 2^31 node limit of one domain", n);
+  if (cfg->length[1] > 65535 || cfg->length[2] > 65535)
+    return fail(LBMC_ERR_UNSUPPORTED, "Ly and Lz are limited to 65535 (one grid row per (y, z))");
+  if (!(cfg->tau > 0.0) || !std::isfinite(cfg->tau))
+    return fail(LBMC_ERR_INVALID_ARG, "tau must be positive and finite (got %g)", cfg->tau);
+  if (cfg->collision_type < 0 || cfg->collision_type > 3)
+    return fail(LBMC_ERR_INVALID_ARG, "unknown collision type %d", cfg->collision_type);
+  if (cfg->c_smag > 0 && cfg->collision_type >= LBMC_MRT)
+    return fail(LBMC_ERR_UNSUPPORTED, "Smagorinsky is only defined for the BGK family (ColType BGK/NTPOR)");
+  if (!(cfg->c_smag >= 0.0) || !std::isfinite(cfg->c_smag))
+    return fail(LBMC_ERR_INVALID_ARG, "c_smag must be >= 0 (got %g)", cfg->c_smag);
+  if (cfg->storage < LBMC_F32 || cfg->storage > LBMC_F64)
+    return fail(LBMC_ERR_INVALID_ARG, "unknown storage %d", cfg->storage);
+  if (cfg->streaming != LBMC_STREAM_SHIFT && cfg->streaming != LBMC_STREAM_AA)
+    return fail(LBMC_ERR_INVALID_ARG, "unknown streaming scheme %d", cfg->streaming);
+  if (cfg->streaming == LBMC_STREAM_AA)
+    return fail(LBMC_ERR_UNSUPPORTED, "AA-pattern streaming is not available in this build");
+  if (cfg->init_type < 0 || cfg->init_type > 2)
+    return fail(LBMC_ERR_INVALID_ARG, "unknown init type %d", cfg->init_type);
+  if (cfg->compat & ~(LBMC_COMPAT_REFERENCE_AS_IS))
+    return fail(LBMC_ERR_INVALID_ARG, "unknown compat bits 0x%x", cfg->compat);
+  if (cfg->storage_scale < 0 || !std::isfinite(cfg->storage_scale))
+    return fail(LBMC_ERR_INVALID_ARG, "storage_scale must be >= 0");
+  if (!dom) return fail(LBMC_ERR_INVALID_ARG, "domain is NULL");
+  if (cfg->init_type == LBMC_INIT_F && !dom->f)
+    return fail(LBMC_ERR_INVALID_ARG, "init_type LBMC_INIT_F needs domain.f");
+  if (cfg->macro_bc && !dom->macro_bc)
+    return fail(LBMC_ERR_INVALID_ARG, "macro_bc is on but domain.macro_bc is NULL");
+  if (cfg->micro_bc && !dom->micro_bc)
+    return fail(LBMC_ERR_INVALID_ARG, "micro_bc is on but domain.micro_bc is NULL");
+  const int q = lattice_q(cfg->lattice);
+  bool needs_rho = false;
+  for (long long k = 0; k < n; k++) {
+    const double B = dom->geometry ? dom->geometry[k] : 0.0;
+    if (!std::isfinite(B)) return fail(LBMC_ERR_INVALID_ARG, "Porosity at node %lld is not finite", k);
+    if (B >= 1) continue;
+    if (cfg->macro_bc) {
+      const int c = dom->macro_bc[k];
+      if (c < 0 || c > 15) return fail(LBMC_ERR_INVALID_ARG, "MacroBC code %d at node %lld is outside 0..15", c, k);
+      if (macro_mask(c) & 0x8) needs_rho = true;
+      if ((macro_mask(c) & 0x7) && !(dom->u[0] && dom->u[1] && (dim == 2 || dom->u[2])))
+        return fail(LBMC_ERR_INVALID_ARG, "MacroBC code %d needs the velocity fields", c);
+    }
+    if (cfg->micro_bc) {
+      const int c = dom->micro_bc[k];
+      const int maxc = cfg->lattice == LBMC_D2Q9 ? 8 : 12;
+      if (c < 0 || c > maxc)
+        return fail(LBMC_ERR_INVALID_ARG, "MicroBC code %d at node %lld is outside 0..%d", c, k, maxc);
+      // micro_bc.cuh:7-8 leaves D2Q9 codes 3 and 4 as NULL entries.
+      if (cfg->lattice == LBMC_D2Q9 && (c == 3 || c == 4))
+        return fail(LBMC_ERR_INVALID_ARG, "MicroBC code %d is undefined for D2Q9 (node %lld)", c, k);
+    }
+  }
+  if (needs_rho && !dom->rho) return fail(LBMC_ERR_INVALID_ARG, "a MacroBC code prescribes rho but domain.rho is NULL");
+  (void)q;
+  return LBMC_OK;
+}
+
+// Packs Porosity / MacroBC / MicroBC into class bytes (host only, no GPU).
+static lbmc_status build_classes(const lbmc_config *cfg, const lbmc_domain *dom, long long n,
+                                 HostClasses &hc) {
+  hc.cls.assign(n, 0);
+  memset(hc.table, 0, sizeof(hc.table));
+  std::map<unsigned, int> ids;
+  const bool blend = cfg->collision_type == LBMC_NTPOR || cfg->collision_type == LBMC_MRTPOR;
+  const int L0 = cfg->length[0], L1 = cfg->length[1];
+  for (long long k = 0; k < n; k++) {
+    const double B = dom->geometry ? dom->geometry[k] : 0.0;
+    if (B >= 1) {  // LBM-C/solver.cu:67-72
+      hc.cls[k] = CLASS_SOLID;
+      continue;
+    }
+    const int macro = cfg->macro_bc ? dom->macro_bc[k] : 0;
+    const int micro = cfg->micro_bc ? dom->micro_bc[k] : 0;
+    const bool partial = blend && B != 0.0;
+    const unsigned entry = (unsigned)macro | ((unsigned)micro << ENTRY_MICRO_SHIFT) | (partial ? ENTRY_PARTIAL : 0u);
+    if (partial) hc.any_partial = true;
+    if (micro && is_sf_code(cfg->lattice, micro)) {
+      const int face = cfg->lattice == LBMC_D2Q9 ? micro - 5 : micro - 7;
+      hc.sf_nodes.push_back((int)k);
+      hc.sf_face.push_back((uint8_t)face);
+    }
+    if (!entry) continue;
+    auto it = ids.find(entry);
+    int id;
+    if (it == ids.end()) {
+      if (hc.nclasses >= 256)
+        return fail(LBMC_ERR_UNSUPPORTED, "more than 254 distinct (MacroBC, MicroBC, partial) combinations");
+      id = hc.nclasses++;
+      ids[entry] = id;
+      hc.table[id] = (uint16_t)entry;
+    } else {
+      id = it->second;
+    }
+    hc.cls[k] = (uint8_t)id;
+  }
+  (void)L0;
+  (void)L1;
+  return LBMC_OK;
+}
+
+// Host-only view of the class packing, for tests and tools.
+extern "C" lbmc_status lbmc_classify(const lbmc_config *cfg, const lbmc_domain *dom,
+                                     uint8_t *cls_out, uint16_t *table_out, int *nclasses) {
+  lbmc_status s = lbmc_validate(cfg, dom);
+  if (s != LBMC_OK) return s;
+  long long n = 1;
+  for (int d = 0; d < lattice_dim(cfg->lattice); d++) n *= cfg->length[d];
+  HostClasses hc;
+  s = build_classes(cfg, dom, n, hc);
+  if (s != LBMC_OK) return s;
+  if (cls_out) memcpy(cls_out, hc.cls.data(), n);
+  if (table_out) memcpy(table_out, hc.table, sizeof(hc.table));
+  if (nclasses) *nclasses = hc.nclasses;
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_lattice_tables(int lattice, int *e, double *w, int *opp, int *m) {
+  if (lattice != LBMC_D2Q9 && lattice != LBMC_D3Q15)
+    return fail(LBMC_ERR_INVALID_ARG, "unknown lattice %d", lattice);
+  const int q = lattice_q(lattice), dim = lattice_dim(lattice);
+  for (int i = 0; i < q; i++) {
+    for (int d = 0; d < dim; d++)
+      if (e) e[d * q + i] = lattice_e(lattice, d, i);
+    if (w) w[i] = lattice_w(lattice, i);
+    if (opp) opp[i] = lattice == LBMC_D2Q9 ? D2Q9::opp(i) : D3Q15::opp(i);
+    for (int k = 0; k < q; k++)
+      if (m) m[k * q + i] = lattice == LBMC_D2Q9 ? D2Q9::m(k, i) : D3Q15::m(k, i);
+  }
+  return LBMC_OK;
+}
+
+// ------------------------------------------------------------ allocation
+
+template <class T>
+static lbmc_status dev_alloc(lbmc_handle *h, T **p, size_t bytes, const char *what) {
+  void *ptr = nullptr;
+  cudaError_t e = cudaMalloc(&ptr, bytes ? bytes : 16);
+  if (e != cudaSuccess) return fail(LBMC_ERR_ALLOC, "cudaMalloc(%zu) for %s: %s", bytes, what, cudaGetErrorString(e));
+  h->allocations.push_back(ptr);
+  *p = static_cast<T *>(ptr);
+  return LBMC_OK;
+}
+
+// Uploads N doubles as the compute type (float or double).
+static lbmc_status upload_compute(lbmc_handle *h, void *dst, const double *src, long long n,
+                                  double offset, double fill) {
+  const int cs = h->ops->csize;
+  if (cs == 8) {
+    std::vector<double> tmp(n);
+    for (long long k = 0; k < n; k++) tmp[k] = src ? src[k] + offset : fill;
+    CK(cudaMemcpy(dst, tmp.data(), n * 8, cudaMemcpyHostToDevice), "upload field");
+  } else {
+    std::vector<float> tmp(n);
+    for (long long k = 0; k < n; k++) tmp[k] = (float)(src ? src[k] + offset : fill);
+    CK(cudaMemcpy(dst, tmp.data(), n * 4, cudaMemcpyHostToDevice), "upload field");
+  }
+  return LBMC_OK;
+}
+
+static void release(lbmc_handle *h) {
+  if (!h) return;
+  for (void *p : h->allocations) cudaFree(p);
+  h->allocations.clear();
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+}
+
+#define TRY(call)                  \
+  do {                             \
+    lbmc_status s_ = (call);       \
+    if (s_ != LBMC_OK) {           \
+      release(h);                  \
+      return s_;                   \
+    }                              \
+  } while (0)
+
+#define TRYCUDA(call, what)                       \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) {                      \
+      lbmc_status s_ = cuda_fail(e_, what);       \
+      release(h);                                 \
+      return s_;                                  \
+    }                                             \
+  } while (0)
+
+extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom, lbmc_handle **out) {
+  if (!out) return fail(LBMC_ERR_INVALID_ARG, "lbmc_init: out is NULL");
+  *out = nullptr;
+  lbmc_status st = lbmc_validate(cfg, dom);
+  if (st != LBMC_OK) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(LBMC_ERR_NO_DEVICE, "no CUDA device is available");
+  }
+  if (cfg->device < 0 || cfg->device >= ndev)
+    return fail(LBMC_ERR_INVALID_ARG, "device %d does not exist (%d devices)", cfg->device, ndev);
+  CK(cudaSetDevice(cfg->device), "cudaSetDevice");
+
+  lbmc_handle *h = new (std::nothrow) lbmc_handle();
+  if (!h) return fail(LBMC_ERR_ALLOC, "host allocation failed");
+  h->cfg = *cfg;
+  DeviceState &d = h->ds;
+  memset(&d, 0, sizeof(d));
+  d.lattice = cfg->lattice;
+  d.storage = cfg->storage;
+  d.q = lattice_q(cfg->lattice);
+  d.dim = lattice_dim(cfg->lattice);
+  d.n = 1;
+  for (int k = 0; k < 3; k++) {
+    d.L[k] = k < d.dim ? cfg->length[k] : 1;
+    d.n *= d.L[k];
+  }
+  h->ops = select_ops(cfg->lattice, cfg->storage);
+  const long long n = d.n;
+  const int q = d.q, cs = h->ops->csize, ss = h->ops->ssize;
+
+  HostClasses hc;
+  TRY(build_classes(cfg, dom, n, hc));
+  memcpy(d.table, hc.table, sizeof(d.table));
+
+  d.tau = cfg->tau;
+  d.c_smag = cfg->c_smag;
+  for (int k = 0; k < 15; k++) d.s_mrt[k] = k < q ? cfg->tau_mrt[k] : 0.0;
+  d.scale = cfg->storage_scale > 0 ? cfg->storage_scale : default_scale(cfg->storage);
+  d.compat = cfg->compat;
+  d.col = cfg->collision_type >= LBMC_MRT ? COL_MRT : (cfg->c_smag > 0 ? COL_BGK_SMAG : COL_BGK);
+  d.forcing = cfg->forcing ? 1 : 0;
+  d.blend = hc.any_partial ? 1 : 0;
+
+  TRYCUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  h->stream = h->own_stream;
+
+  // Populations: Q arrays, each padded to a 256-byte boundary.
+  const long long align = 256 / ss;
+  d.pitch = (n + align - 1) / align * align;
+  TRY(dev_alloc(h, &d.f, (size_t)d.pitch * q * ss, "populations"));
+  TRY(dev_alloc(h, &d.cls, (size_t)n, "node classes"));
+  TRYCUDA(cudaMemcpy(d.cls, hc.cls.data(), n, cudaMemcpyHostToDevice), "upload classes");
+
+  // rho - 1 and u: prescribed input (macro BC) and stored output.
+  TRY(dev_alloc(h, &d.rho, (size_t)n * cs, "rho"));
+  TRY(upload_compute(h, d.rho, dom->rho, n, -1.0, 0.0));
+  for (int k = 0; k < 3; k++) {
+    if (k < d.dim) {
+      TRY(dev_alloc(h, &d.u[k], (size_t)n * cs, "u"));
+      TRY(upload_compute(h, d.u[k], dom->u[k], n, 0.0, 0.0));
+    }
+  }
+  if (d.dim == 2) d.u[2] = d.u[1];  // never written for D2Q9; keeps pointers valid
+
+  if (hc.any_partial) {
+    TRY(dev_alloc(h, &d.B, (size_t)n * cs, "porosity"));
+    TRY(upload_compute(h, d.B, dom->geometry, n, 0.0, 0.0));
+  }
+
+  if (cfg->forcing) {
+    bool uniform = true;
+    for (int k = 0; k < d.dim && uniform; k++) {
+      const double *F = dom->force[k];
+      const double v0 = F ? F[0] : 0.0;
+      d.force_u[k] = v0;
+      if (F)
+        for (long long j = 1; j < n; j++)
+          if (F[j] != v0) {
+            uniform = false;
+            break;
+          }
+    }
+    if (!uniform) {
+      for (int k = 0; k < d.dim; k++) {
+        TRY(dev_alloc(h, &d.force[k], (size_t)n * cs, "force"));
+        TRY(upload_compute(h, d.force[k], dom->force[k], n, 0.0, 0.0));
+      }
+      if (d.dim == 2) d.force[2] = d.force[1];
+      d.force_u[0] = d.force_u[1] = d.force_u[2] = 0;
+    }
+  }
+
+  if (!hc.sf_nodes.empty()) {
+    d.n_sf = (int)hc.sf_nodes.size();
+    TRY(dev_alloc(h, &d.sf_nodes, sizeof(int) * d.n_sf, "sf nodes"));
+    TRY(dev_alloc(h, &d.sf_face, d.n_sf, "sf faces"));
+    TRY(dev_alloc(h, &d.sf_index, sizeof(int) * n, "sf index"));
+    TRY(dev_alloc(h, &d.sf_buf, (size_t)cs * q * d.n_sf, "sf buffer"));
+    std::vector<int> idx(n, -1);
+    for (int k = 0; k < d.n_sf; k++) idx[hc.sf_nodes[k]] = k;
+    TRYCUDA(cudaMemcpy(d.sf_nodes, hc.sf_nodes.data(), sizeof(int) * d.n_sf, cudaMemcpyHostToDevice), "upload sf");
+    TRYCUDA(cudaMemcpy(d.sf_face, hc.sf_face.data(), d.n_sf, cudaMemcpyHostToDevice), "upload sf");
+    TRYCUDA(cudaMemcpy(d.sf_index, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload sf");
+    TRYCUDA(cudaMemset(d.sf_buf, 0, (size_t)cs * q * d.n_sf), "clear sf");
+  }
+
+  h->nblocks = h->ops->step_blocks(d);
+  TRY(dev_alloc(h, &d.partials, sizeof(double) * DIAG_VALUES * h->nblocks, "diagnostic partials"));
+  TRY(dev_alloc(h, &d.flag, sizeof(unsigned), "diagnostic flag"));
+  TRY(dev_alloc(h, &h->diag_out, sizeof(double) * DIAG_VALUES, "diagnostics"));
+  TRYCUDA(cudaMemset(d.flag, 0, sizeof(unsigned)), "clear flag");
+
+  // Initial populations (Init: model_builder.cu:227-248 for Init 0).
+  if (cfg->init_type == LBMC_INIT_STATIC) {
+    TRYCUDA(cudaMemset(d.f, 0, (size_t)d.pitch * q * ss), "clear populations");
+  } else {
+    double *tmp = nullptr;
+    TRYCUDA(cudaMalloc(&tmp, sizeof(double) * n), "init staging");
+    std::vector<double> host(n);
+    lbmc_status s2 = LBMC_OK;
+    for (int i = 0; i < q && s2 == LBMC_OK; i++) {
+      if (cfg->init_type == LBMC_INIT_F) {
+        memcpy(host.data(), dom->f + (size_t)i * n, sizeof(double) * n);
+      } else {
+        // f_eq(rho, u) of collision.cu:58.
+        const double w = lattice_w(d.lattice, i);
+        for (long long k = 0; k < n; k++) {
+          const double rho = dom->rho ? dom->rho[k] : 1.0;
+          double u[3] = {0, 0, 0}, usq = 0, eu = 0;
+          for (int c = 0; c < d.dim; c++) {
+            u[c] = dom->u[c] ? dom->u[c][k] : 0.0;
+            usq += u[c] * u[c];
+            eu += lattice_e(d.lattice, c, i) * u[c];
+          }
+          eu *= 3.0;
+          host[k] = rho * w * (1.0 + eu + 0.5 * eu * eu - 1.5 * usq);
+        }
+      }
+      cudaError_t e = cudaMemcpy(tmp, host.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = h->ops->upload_population(d, 0, i, tmp, h->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+      if (e != cudaSuccess) s2 = cuda_fail(e, "upload initial populations");
+    }
+    cudaFree(tmp);
+    if (s2 != LBMC_OK) {
+      release(h);
+      return s2;
+    }
+  }
+  TRYCUDA(cudaDeviceSynchronize(), "lbmc_init");
+  *out = h;
+  return LBMC_OK;
+}
+
+// Sums the per-block partials in FP64 in a fixed order (deterministic).
+__global__ void diag_finalize_kernel(const double *partials, long long nblocks, double *out) {
+  __shared__ double sh[256];
+  for (int v = 0; v < DIAG_VALUES; v++) {
+    double acc = 0;
+    for (long long b = threadIdx.x; b < nblocks; b += blockDim.x) acc += partials[b * DIAG_VALUES + v];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[v] = sh[0];
+    __syncthreads();
+  }
+}
+
+extern "C" lbmc_status lbmc_iterate(lbmc_handle *h, int nsteps, unsigned flags) {
+  if (!h) return fail(LBMC_ERR_INVALID_ARG, "lbmc_iterate: handle is NULL");
+  if (nsteps < 0) return fail(LBMC_ERR_INVALID_ARG, "lbmc_iterate: nsteps = %d", nsteps);
+  if (flags & ~(LBMC_STORE_MACROS | LBMC_REDUCE_DIAG | LBMC_SYNC))
+    return fail(LBMC_ERR_INVALID_ARG, "lbmc_iterate: unknown flags 0x%x", flags);
+  CK(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  for (int s = 0; s < nsteps; s++) {
+    const bool last = s == nsteps - 1;
+    const bool store = last && (flags & LBMC_STORE_MACROS);
+    const bool diag = last && (flags & LBMC_REDUCE_DIAG);
+    if (diag) CK(cudaMemsetAsync(h->ds.flag, 0, sizeof(unsigned), h->stream), "clear flag");
+    CK(h->ops->step(h->ds, h->step, store, diag, h->stream), "step kernel launch");
+    h->step++;
+    if (diag) {
+      diag_finalize_kernel<<<1, 256, 0, h->stream>>>(h->ds.partials, h->nblocks, h->diag_out);
+      CK(cudaGetLastError(), "diagnostic reduction launch");
+      h->diag_step = h->step;
+    }
+  }
+  if (flags & LBMC_SYNC) {
+    CK(cudaStreamSynchronize(h->stream), "lbmc_iterate");
+    if ((flags & LBMC_REDUCE_DIAG) && nsteps > 0) {
+      unsigned flag = 0;
+      CK(cudaMemcpy(&flag, h->ds.flag, sizeof(flag), cudaMemcpyDeviceToHost), "read flag");
+      if (flag) return fail(LBMC_ERR_NAN, "non-finite density or velocity at step %lld", h->step);
+    }
+  }
+  return LBMC_OK;
+}
+
+static lbmc_status fetch_compute(lbmc_handle *h, const void *src, double *dst, long long n, double offset) {
+  if (h->ops->csize == 8) {
+    CK(cudaMemcpy(dst, src, n * 8, cudaMemcpyDeviceToHost), "fetch field");
+    if (offset != 0)
+      for (long long k = 0; k < n; k++) dst[k] += offset;
+  } else {
+    std::vector<float> tmp(n);
+    CK(cudaMemcpy(tmp.data(), src, n * 4, cudaMemcpyDeviceToHost), "fetch field");
+    for (long long k = 0; k < n; k++) dst[k] = (double)tmp[k] + offset;
+  }
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_fetch(lbmc_handle *h, int field, void *dst, size_t bytes) {
+  if (!h) return fail(LBMC_ERR_INVALID_ARG, "lbmc_fetch: handle is NULL");
+  if (!dst) return fail(LBMC_ERR_INVALID_ARG, "lbmc_fetch: dst is NULL");
+  CK(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(h->stream), "lbmc_fetch");
+  const DeviceState &d = h->ds;
+  const long long n = d.n;
+  switch (field) {
+    case LBMC_FIELD_RHO:
+    case LBMC_FIELD_U_X:
+    case LBMC_FIELD_U_Y:
+    case LBMC_FIELD_U_Z: {
+      if (bytes < (size_t)n * 8) return fail(LBMC_ERR_BUFFER_SIZE, "lbmc_fetch: need %lld bytes", n * 8);
+      if (field == LBMC_FIELD_U_Z && d.dim == 2)
+        return fail(LBMC_ERR_INVALID_ARG, "lbmc_fetch: D2Q9 has no z velocity");
+      const void *src = field == LBMC_FIELD_RHO ? d.rho : d.u[field - LBMC_FIELD_U_X];
+      return fetch_compute(h, src, static_cast<double *>(dst), n, field == LBMC_FIELD_RHO ? 1.0 : 0.0);
+    }
+    case LBMC_FIELD_F: {
+      if (bytes < (size_t)n * d.q * 8)
+        return fail(LBMC_ERR_BUFFER_SIZE, "lbmc_fetch: need %lld bytes", n * d.q * 8);
+      double *tmp = nullptr;
+      CK(cudaMalloc(&tmp, sizeof(double) * n), "fetch staging");
+      cudaError_t e = cudaSuccess;
+      for (int i = 0; i < d.q && e == cudaSuccess; i++) {
+        e = h->ops->fetch_population(d, h->step, i, tmp, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e == cudaSuccess)
+          e = cudaMemcpy(static_cast<double *>(dst) + (size_t)i * n, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost);
+      }
+      cudaFree(tmp);
+      if (e != cudaSuccess) return cuda_fail(e, "lbmc_fetch populations");
+      return LBMC_OK;
+    }
+    case LBMC_FIELD_DIAG: {
+      if (bytes < sizeof(lbmc_diag)) return fail(LBMC_ERR_BUFFER_SIZE, "lbmc_fetch: need sizeof(lbmc_diag)");
+      lbmc_diag out;
+      memset(&out, 0, sizeof(out));
+      if (h->diag_step >= 0) {
+        double v[DIAG_VALUES];
+        unsigned flag = 0;
+        CK(cudaMemcpy(v, h->diag_out, sizeof(v), cudaMemcpyDeviceToHost), "fetch diagnostics");
+        CK(cudaMemcpy(&flag, d.flag, sizeof(flag), cudaMemcpyDeviceToHost), "fetch diagnostics");
+        out.mass = v[0];
+        out.momentum[0] = v[1];
+        out.momentum[1] = v[2];
+        out.momentum[2] = v[3];
+        out.kinetic_energy = v[4];
+        out.step = h->diag_step;
+        out.nonfinite = flag ? 1 : 0;
+        out.valid = 1;
+      }
+      memcpy(dst, &out, sizeof(out));
+      return LBMC_OK;
+    }
+    default:
+      return fail(LBMC_ERR_INVALID_ARG, "lbmc_fetch: unknown field %d", field);
+  }
+}
+
+extern "C" lbmc_status lbmc_destroy(lbmc_handle *h) {
+  if (!h) return LBMC_OK;
+  cudaSetDevice(h->cfg.device);
+  cudaStreamSynchronize(h->stream);
+  release(h);
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_get_step(lbmc_handle *h, long long *step) {
+  if (!h || !step) return fail(LBMC_ERR_INVALID_ARG, "lbmc_get_step: NULL argument");
+  *step = h->step;
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_set_stream(lbmc_handle *h, void *cuda_stream) {
+  if (!h) return fail(LBMC_ERR_INVALID_ARG, "lbmc_set_stream: handle is NULL");
+  CK(cudaStreamSynchronize(h->stream), "lbmc_set_stream");
+  h->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : h->own_stream;
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_synchronize(lbmc_handle *h) {
+  if (!h) return fail(LBMC_ERR_INVALID_ARG, "lbmc_synchronize: handle is NULL");
+  CK(cudaStreamSynchronize(h->stream), "lbmc_synchronize");
+  return LBMC_OK;
+}
+
+extern "C" const char *lbmc_status_string(lbmc_status s) {
+  switch (s) {
+    case LBMC_OK: return "ok";
+    case LBMC_ERR_INVALID_ARG: return "invalid argument";
+    case LBMC_ERR_UNSUPPORTED: return "unsupported";
+    case LBMC_ERR_CUDA: return "CUDA error";
+    case LBMC_ERR_ALLOC: return "allocation failed";
+    case LBMC_ERR_NAN: return "non-finite value";
+    case LBMC_ERR_TIMEOUT: return "timeout";
+    case LBMC_ERR_IO: return "I/O error";
+    case LBMC_ERR_BUFFER_SIZE: return "buffer too small";
+    case LBMC_ERR_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+extern "C" const char *lbmc_last_error(void) { return g_last_error.c_str(); }

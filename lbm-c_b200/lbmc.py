@@ -1,0 +1,268 @@
+"""ctypes binding of the lbmc C ABI (include/lbmc.h).
+
+This is the Python mirror of the engine's drop-in boundary: ``Engine`` wraps
+``lbmc_init`` / ``lbmc_iterate`` / ``lbmc_fetch`` / ``lbmc_destroy`` exactly,
+with the same argument meaning and status codes (errors raise ``LbmcError``
+carrying the status and ``lbmc_last_error()``).  It loads the in-tree
+``liblbmc.so`` built by ``make -C lbm-c_b200`` and fails loudly when that
+library is absent: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbmc.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "lbmc.h")
+
+# enums / flags of include/lbmc.h
+OK, ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_ALLOC, ERR_NAN, ERR_TIMEOUT, ERR_IO, \
+    ERR_BUFFER_SIZE, ERR_NO_DEVICE = range(10)
+D2Q9, D3Q15 = 0, 1
+F32, F16, BF16, F64 = 0, 1, 2, 3
+BGK, NTPOR, MRT, MRTPOR = 0, 1, 2, 3
+INIT_STATIC, INIT_EQUILIBRIUM, INIT_F = 0, 1, 2
+STREAM_SHIFT, STREAM_AA = 0, 1
+COMPAT_D3Q15_MINV_ZERO = 1 << 0
+COMPAT_MEQ_INT_DIV = 1 << 1
+COMPAT_ZH_Z_UX = 1 << 2
+COMPAT_MRTPOR_INPLACE = 1 << 3
+COMPAT_REFERENCE_AS_IS = 0xF
+STORE_MACROS, REDUCE_DIAG, SYNC = 1, 2, 4
+FIELD_RHO, FIELD_U_X, FIELD_U_Y, FIELD_U_Z, FIELD_F, FIELD_DIAG = range(6)
+
+LATTICE_IDS = {"d2q9": D2Q9, "d3q15": D3Q15}
+STORAGE_IDS = {"f32": F32, "f16": F16, "bf16": BF16, "f64": F64}
+
+_P = ctypes.c_void_p
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("lattice", ctypes.c_int), ("length", ctypes.c_int * 3),
+                ("tau", ctypes.c_double), ("tau_mrt", ctypes.c_double * 15),
+                ("c_smag", ctypes.c_double), ("collision_type", ctypes.c_int),
+                ("forcing", ctypes.c_int), ("macro_bc", ctypes.c_int),
+                ("micro_bc", ctypes.c_int), ("init_type", ctypes.c_int),
+                ("tolerance", ctypes.c_double), ("h", ctypes.c_int), ("dt", ctypes.c_int),
+                ("storage", ctypes.c_int), ("streaming", ctypes.c_int),
+                ("compat", ctypes.c_uint), ("storage_scale", ctypes.c_double),
+                ("device", ctypes.c_int), ("block_size", ctypes.c_int),
+                ("reserved", ctypes.c_int * 6)]
+
+
+class Domain(ctypes.Structure):
+    _fields_ = [("geometry", _DP), ("force", _DP * 3), ("macro_bc", _IP),
+                ("micro_bc", _IP), ("u", _DP * 3), ("rho", _DP), ("f", _DP)]
+
+
+class Diag(ctypes.Structure):
+    _fields_ = [("mass", ctypes.c_double), ("momentum", ctypes.c_double * 3),
+                ("kinetic_energy", ctypes.c_double), ("step", ctypes.c_longlong),
+                ("nonfinite", ctypes.c_int), ("valid", ctypes.c_int)]
+
+
+class LbmcError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"lbmc status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """The in-tree liblbmc.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C lbm-c_b200` "
+                               "(the engine has no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.lbmc_config_default.argtypes = [ctypes.POINTER(Config), ctypes.c_int]
+        lib.lbmc_validate.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(Domain)]
+        lib.lbmc_init.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(Domain),
+                                  ctypes.POINTER(_P)]
+        lib.lbmc_iterate.argtypes = [_P, ctypes.c_int, ctypes.c_uint]
+        lib.lbmc_fetch.argtypes = [_P, ctypes.c_int, _P, ctypes.c_size_t]
+        lib.lbmc_destroy.argtypes = [_P]
+        lib.lbmc_get_step.argtypes = [_P, ctypes.POINTER(ctypes.c_longlong)]
+        lib.lbmc_set_stream.argtypes = [_P, _P]
+        lib.lbmc_synchronize.argtypes = [_P]
+        lib.lbmc_status_string.restype = ctypes.c_char_p
+        lib.lbmc_status_string.argtypes = [ctypes.c_int]
+        lib.lbmc_last_error.restype = ctypes.c_char_p
+        lib.lbmc_last_error.argtypes = []
+        lib.lbmc_classify.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(Domain), _P, _P,
+                                      ctypes.POINTER(ctypes.c_int)]
+        lib.lbmc_lattice_tables.argtypes = [ctypes.c_int, _P, _P, _P, _P]
+        for name in ("lbmc_config_default", "lbmc_validate", "lbmc_init", "lbmc_iterate",
+                     "lbmc_fetch", "lbmc_destroy", "lbmc_get_step", "lbmc_set_stream",
+                     "lbmc_synchronize", "lbmc_classify", "lbmc_lattice_tables"):
+            getattr(lib, name).restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def check(status: int):
+    if status != OK:
+        raise LbmcError(status, library().lbmc_last_error().decode())
+
+
+def header_functions(path: str = HEADER) -> list[str]:
+    """Names of the functions include/lbmc.h declares."""
+    import re
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lbmc_[a-z_]+)\s*\(", text)))
+
+
+def _as_f64(a, n):
+    return None if a is None else np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1)[:n])
+
+
+class _Keep:
+    """Holds the numpy arrays a Domain points into."""
+
+    def __init__(self):
+        self.arrays = []
+
+    def ptr_d(self, a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, np.float64)
+        self.arrays.append(a)
+        return a.ctypes.data_as(_DP)
+
+    def ptr_i(self, a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, np.int32)
+        self.arrays.append(a)
+        return a.ctypes.data_as(_IP)
+
+
+def make_config(lattice, length, tau=1.0, tau_mrt=(), c_smag=0.0, collision_type=BGK,
+                forcing=False, macro_bc=False, micro_bc=False, init_type=INIT_STATIC,
+                storage=F32, compat=0, storage_scale=0.0, device=0, streaming=STREAM_SHIFT,
+                tolerance=0.0) -> Config:
+    lat = LATTICE_IDS.get(lattice, lattice)
+    cfg = Config()
+    check(library().lbmc_config_default(ctypes.byref(cfg), lat))
+    for d in range(3):
+        cfg.length[d] = int(length[d]) if d < len(length) else 1
+    if lat == D2Q9:
+        cfg.length[2] = 1
+    cfg.tau = tau
+    for i, v in enumerate(tau_mrt):
+        cfg.tau_mrt[i] = v
+    cfg.c_smag = c_smag
+    cfg.collision_type = collision_type
+    cfg.forcing = int(bool(forcing))
+    cfg.macro_bc = int(bool(macro_bc))
+    cfg.micro_bc = int(bool(micro_bc))
+    cfg.init_type = init_type
+    cfg.storage = STORAGE_IDS.get(storage, storage)
+    cfg.compat = compat
+    cfg.storage_scale = storage_scale
+    cfg.device = device
+    cfg.streaming = streaming
+    cfg.tolerance = tolerance
+    return cfg
+
+
+def make_domain(n, dim, q, geometry=None, force=None, macro=None, micro=None, u=None,
+                rho=None, f=None):
+    keep = _Keep()
+    dom = Domain()
+    dom.geometry = keep.ptr_d(geometry)
+    for d in range(3):
+        dom.force[d] = keep.ptr_d(None if force is None or d >= dim else np.asarray(force)[d])
+        dom.u[d] = keep.ptr_d(None if u is None or d >= dim else np.asarray(u)[d])
+    dom.macro_bc = keep.ptr_i(macro)
+    dom.micro_bc = keep.ptr_i(micro)
+    dom.rho = keep.ptr_d(rho)
+    dom.f = keep.ptr_d(f)
+    return dom, keep
+
+
+class Engine:
+    """One lbmc handle: ``Engine(cfg, domain)`` = lbmc_init."""
+
+    def __init__(self, cfg: Config, dom: Domain):
+        lib = library()
+        self.cfg = cfg
+        self.dim = 2 if cfg.lattice == D2Q9 else 3
+        self.q = 9 if cfg.lattice == D2Q9 else 15
+        self.n = int(np.prod([cfg.length[d] for d in range(self.dim)]))
+        h = _P()
+        check(lib.lbmc_init(ctypes.byref(cfg), ctypes.byref(dom), ctypes.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_case(cls, case, storage=F32, init_type=None, compat=None, **kw):
+        """Builds an engine for an oracle ``Case`` (tests/cases.py)."""
+        a = case.arrays()
+        if init_type is None:
+            init_type = INIT_F if a["f0"] is not None else INIT_STATIC
+        cfg = make_config(case.lattice, case.length, tau=case.tau, tau_mrt=case.tau_mrt,
+                          c_smag=case.c_smag, collision_type=case.collision_type,
+                          forcing=case.forcing, macro_bc=case.macro_bc,
+                          micro_bc=case.micro_bc, init_type=init_type, storage=storage,
+                          compat=case.compat if compat is None else compat, **kw)
+        dom, keep = make_domain(case.n, case.dim, case.q, a["geometry"], a["force"], a["macro"],
+                                a["micro"], a["u"], a["rho"], a["f0"])
+        eng = cls(cfg, dom)
+        del keep
+        return eng
+
+    def iterate(self, nsteps: int, flags: int = 0):
+        check(library().lbmc_iterate(self.h, nsteps, flags))
+
+    def _fetch(self, field, out):
+        check(library().lbmc_fetch(self.h, field, out.ctypes.data_as(_P), out.nbytes))
+        return out
+
+    def rho(self):
+        return self._fetch(FIELD_RHO, np.empty(self.n))
+
+    def u(self):
+        return np.stack([self._fetch(FIELD_U_X + d, np.empty(self.n)) for d in range(self.dim)])
+
+    def f(self):
+        return self._fetch(FIELD_F, np.empty((self.q, self.n)))
+
+    def diag(self) -> Diag:
+        d = Diag()
+        check(library().lbmc_fetch(self.h, FIELD_DIAG, ctypes.cast(ctypes.byref(d), _P),
+                                   ctypes.sizeof(d)))
+        return d
+
+    def step(self) -> int:
+        v = ctypes.c_longlong()
+        check(library().lbmc_get_step(self.h, ctypes.byref(v)))
+        return v.value
+
+    def synchronize(self):
+        check(library().lbmc_synchronize(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            library().lbmc_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
