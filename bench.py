@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark of the fused LBM time step on B200.
+
+Workload (the configuration the headline metric is quoted on): D3Q15 MRT
+porous medium, 256^3 nodes, FP32 population storage, overlapping spheres
+(radius 6) at solid fraction 0.30 with full-way bounceback, Zou-He pressure
+faces rho = 1.001 / 0.999 on x, periodic y/z, tau = 0.7, s_e = s_eps = 1.19,
+s_q = s_m = 1.2, s_nu = 1/tau.  Inputs are seeded synthetic arrays of that
+shape; populations (1 GB) exceed the 126 MB L2, so no flush is needed
+between steps.
+
+One bench step = one LBM time step over the whole domain (one launch of the
+fused step kernel).  value = lattice updates per second (GLUPS) over all
+ranks, timed with CUDA events on the engine's stream, max over ranks.
+e2e = the same metric through the C ABI with host buffers: lbmc_init from
+host arrays (host->device copies), E2E_STEPS time steps, lbmc_fetch of rho
+and u (device->host), lbmc_destroy, per e2e step.
+
+--impl reference times the reference's own step (host-compiled from its
+sources, oracle/_ref) on the host cores with all threads, on a z-crop of the
+same workload.  Multi-GPU: independent replicas (the reference is one GPU,
+one domain), so scaling is weak and there is no collective in the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lbm-c_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "GLUPS (D3Q15 MRT porous 256^3 fused step)"
+UNIT = "GLUPS"
+E2E_STEPS = 500
+STORAGE_BYTES = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}
+
+
+def algorithmic_bytes_per_lup(q: int, storage: str) -> int:
+    """One read and one write of every population plus the class byte."""
+    return 2 * q * STORAGE_BYTES[storage] + 1
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_tag: str):
+    """dram read+write bytes per launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_tag}.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, maxmhz, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                maxmhz.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not mhz:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxmhz),
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def dist_max(value: float, world: int, device=None) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int, device=None):
+    if world > 1:
+        import torch.distributed as dist
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+def build_workload(args):
+    import workloads
+    L = (args.size, args.size, args.size)
+    return workloads.porous_spheres(L)
+
+
+# --------------------------------------------------------------- CPU legs
+
+class ReferenceTimer:
+    """The host-compiled reference step on a z-crop of the workload."""
+
+    def __init__(self, w, nz: int, threads: int):
+        from oracle.oracle import Case, Reference
+        lx, ly, lz = w.length
+        nz = max(1, min(nz, lz))
+        n = lx * ly * nz
+        a = w.arrays
+        case = Case(lattice="d3q15", length=(lx, ly, nz), tau=w.tau, tau_mrt=w.tau_mrt,
+                    collision_type=w.collision_type, macro_bc=True, micro_bc=True,
+                    geometry=a["geometry"][:n], macro=a["macro"][:n], micro=a["micro"][:n],
+                    rho=a["rho"][:n], u=a["u"][:, :n])
+        self.ref = Reference(case, "patched", nthreads=threads)
+        self.n, self.threads = n, threads
+        self.sample = f"{lx}x{ly}x{nz} z-crop of the workload, FP64, patched reference step"
+
+    def rate(self, steps: int) -> float:
+        """Lattice updates per second over `steps` reference steps."""
+        t = time.perf_counter()
+        self.ref.run(steps)
+        return self.n * steps / (time.perf_counter() - t)
+
+    def close(self):
+        self.ref.close()
+
+
+def cpu_reference_rate(w, nz: int, budget_s: float, threads: int):
+    """Reference steps on the crop until about budget_s seconds of CPU work."""
+    timer = ReferenceTimer(w, nz, threads)
+    timer.rate(1)  # page-in
+    steps, t_total = 0, 0.0
+    while t_total < budget_s and steps < 1000:
+        t = time.perf_counter()
+        timer.ref.run(1)
+        t_total += time.perf_counter() - t
+        steps += 1
+    timer.close()
+    return timer.n * steps / t_total, f"{timer.sample}, {steps} steps ({t_total:.1f} s)"
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    w = build_workload(args)
+    threads = os.cpu_count() or 1
+    timer = ReferenceTimer(w, args.ref_nz, threads)
+    timer.rate(max(1, args.warmup))
+    t_total, steps = 0.0, 0
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        timer.ref.run(1)
+        t_total += time.perf_counter() - t
+        steps += 1
+    timer.close()
+    value = timer.n * steps / t_total / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded sphere pack)", "impl": "reference",
+        "config": {"workload": f"porous_spheres_d3q15_mrt_{args.size}^3",
+                   "sample": timer.sample, "storage": "f64", "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{timer.sample}, {steps} steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import lbmc
+    import workloads
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    w = build_workload(args)
+    q = w.q
+    stream = torch.cuda.Stream(device)
+    eng = workloads.engine_for(lbmc, w, args.storage, device=local)
+    lbmc.check(lbmc.library().lbmc_set_stream(eng.h, stream.cuda_stream))
+    # warm-up
+    eng.iterate(args.warmup, lbmc.SYNC)
+    dist_barrier(world, device)
+    torch.cuda.synchronize(device)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        eng.iterate(args.steps, 0)
+        stop.record(stream)
+        stop.synchronize()
+    torch.cuda.synchronize(device)
+    dist_barrier(world, device)
+    ms = start.elapsed_time(stop)
+    ms_max = dist_max(ms, world, device)
+    lups = w.n * args.steps * world
+    value = lups / (ms_max / 1e3) / 1e9
+    eng.iterate(1, lbmc.REDUCE_DIAG | lbmc.SYNC)
+    diag = eng.diag()
+    eng.close()
+
+    # Roofline of the dominant kernel (the fused step): algorithmic bytes per
+    # launch over the average launch time in the timed region.
+    bpl = algorithmic_bytes_per_lup(q, args.storage)
+    per_launch_s = (ms / 1e3) / args.steps
+    achieved = w.n * bpl / per_launch_s / 1e9
+    peak, peak_kind = measured_peak()
+    tag = f"step_kernel_porous{args.size}_{args.storage}"
+    traffic = profiled_traffic(tag)
+
+    # End to end through the C ABI with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        times = []
+        h2d = w.host_bytes()
+        d2h = w.n * 8 * (1 + w.dim)
+        for k in range(args.e2e_reps + 1):
+            torch.cuda.synchronize(device)
+            t = time.perf_counter()
+            e = workloads.engine_for(lbmc, w, args.storage, device=local)
+            e.iterate(E2E_STEPS, lbmc.STORE_MACROS | lbmc.SYNC)
+            e.rho()
+            e.u()
+            e.close()
+            dt = time.perf_counter() - t
+            if k > 0:
+                times.append(dt)
+        t_e2e = dist_max(max(times), world, device)
+        e2e = {"value": w.n * E2E_STEPS * world / t_e2e / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "job": f"lbmc_init from host arrays + {E2E_STEPS} steps + fetch rho,u + destroy"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, sample = cpu_reference_rate(w, args.ref_nz, args.cpu_seconds, threads)
+        cpu = {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "reference",
+               "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.storage, "data": "synthetic (seeded sphere pack)",
+            "config": {"workload": f"porous_spheres_d3q15_mrt_{args.size}^3",
+                       "nodes": w.n, "storage": args.storage, "compute": "f32" if args.storage != "f64" else "f64",
+                       "solid_fraction": round(w.params["solid_fraction"], 4),
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "bytes_per_lup": bpl, "kernel": "step_kernel (fused stream+BC+collide)"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "diag": {"mass": diag.mass, "kinetic_energy": diag.kinetic_energy,
+                     "nonfinite": diag.nonfinite},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--storage", choices=list(STORAGE_BYTES), default="f32")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--e2e-reps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--ref-nz", type=int, default=32)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
