@@ -249,7 +249,9 @@ def run_ours(args, world, rank, local):
     w = build_workload(args)
     q = w.q
     stream = torch.cuda.Stream(device)
-    eng = workloads.engine_for(lbmc, w, args.storage, device=local)
+    kernel = {"auto": lbmc.KERNEL_AUTO, "direct": lbmc.KERNEL_DIRECT,
+              "pipelined": lbmc.KERNEL_PIPELINED}[args.kernel]
+    eng = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel)
     lbmc.check(lbmc.library().lbmc_set_stream(eng.h, stream.cuda_stream))
     # warm-up
     eng.iterate(args.warmup, lbmc.SYNC)
@@ -278,6 +280,8 @@ def run_ours(args, world, rank, local):
     achieved = w.n * bpl / per_launch_s / 1e9
     peak, peak_kind = measured_peak()
     tag = f"step_kernel_porous{args.size}_{args.storage}"
+    if args.kernel != "direct":
+        tag = f"step_pipelined_kernel_porous{args.size}_{args.storage}"
     traffic = profiled_traffic(tag)
 
     # End to end through the C ABI with host buffers.
@@ -289,7 +293,7 @@ def run_ours(args, world, rank, local):
         for k in range(args.e2e_reps + 1):
             torch.cuda.synchronize(device)
             t = time.perf_counter()
-            e = workloads.engine_for(lbmc, w, args.storage, device=local)
+            e = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel)
             e.iterate(E2E_STEPS, lbmc.STORE_MACROS | lbmc.SYNC)
             e.rho()
             e.u()
@@ -322,7 +326,10 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
-                         "bytes_per_lup": bpl, "kernel": "step_kernel (fused stream+BC+collide)"},
+                         "bytes_per_lup": bpl,
+                         "kernel": ("step_pipelined_kernel (bulk-copy row pipeline, fused stream+BC+collide)"
+                                    if args.kernel != "direct" else
+                                    "step_kernel (direct loads, fused stream+BC+collide)")},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
@@ -336,11 +343,12 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--storage", choices=list(STORAGE_BYTES), default="f32")
     ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--kernel", choices=["auto", "direct", "pipelined"], default="auto")
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

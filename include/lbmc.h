@@ -121,9 +121,19 @@ typedef struct lbmc_config {
   unsigned compat;      /* LBMC_COMPAT_* bits */
   double storage_scale; /* stored value = (f - w) * scale; 0 selects the default */
   int device;           /* CUDA device ordinal */
-  int block_size;       /* threads per block of the step kernel; 0 = tuned default */
-  int reserved[6];
+  int block_size;       /* reserved for tuning (0) */
+  int kernel;           /* lbmc_kernel: 0 auto, 1 direct loads, 2 bulk-copy pipeline */
+  int reserved[5];
 } lbmc_config;
+
+/* Step-kernel choice (lbmc_config.kernel).  AUTO takes the bulk-copy
+ * pipeline whenever a row of one population is a whole number of 16-byte
+ * granules and fits the shared-memory stages, else the direct-load kernel. */
+typedef enum lbmc_kernel {
+  LBMC_KERNEL_AUTO = 0,
+  LBMC_KERNEL_DIRECT = 1,
+  LBMC_KERNEL_PIPELINED = 2
+} lbmc_kernel;
 
 /* Host arrays in ixd order; the caller keeps ownership, lbmc_init copies.
  * Mirrors Domain (LBM-C/data_types.cuh:13-21) plus the initial state. */
@@ -194,6 +204,14 @@ lbmc_status lbmc_set_stream(lbmc_handle *h, void *cuda_stream);
 lbmc_status lbmc_synchronize(lbmc_handle *h);
 
 const char *lbmc_status_string(lbmc_status s);
+
+/* Failure-detection self-test: launches a kernel whose bounded wait on a
+ * barrier that is never signalled gives up after `seconds` (<= 10) and
+ * returns LBMC_ERR_TIMEOUT; the context stays usable.  The bulk-copy step
+ * kernel uses the same bounded wait and reports LBMC_ERR_TIMEOUT from
+ * lbmc_iterate(..., LBMC_SYNC) the same way.  No counterpart in the
+ * reference, which has no device-side waits. */
+lbmc_status lbmc_selftest_wait_timeout(int device, double seconds);
 
 /* Host-only helpers (no GPU needed). */
 

@@ -171,6 +171,8 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     return fail(LBMC_ERR_INVALID_ARG, "unknown compat bits 0x%x", cfg->compat);
   if (cfg->storage_scale < 0 || !std::isfinite(cfg->storage_scale))
     return fail(LBMC_ERR_INVALID_ARG, "storage_scale must be >= 0");
+  if (cfg->kernel < LBMC_KERNEL_AUTO || cfg->kernel > LBMC_KERNEL_PIPELINED)
+    return fail(LBMC_ERR_INVALID_ARG, "unknown kernel choice %d", cfg->kernel);
   if (!dom) return fail(LBMC_ERR_INVALID_ARG, "domain is NULL");
   if (cfg->init_type == LBMC_INIT_F && !dom->f)
     return fail(LBMC_ERR_INVALID_ARG, "init_type LBMC_INIT_F needs domain.f");
@@ -443,7 +445,23 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     TRYCUDA(cudaMemset(d.sf_buf, 0, (size_t)cs * q * d.n_sf), "clear sf");
   }
 
-  h->nblocks = h->ops->step_blocks(d);
+  TRY(dev_alloc(h, &d.error_flag, sizeof(unsigned), "error flag"));
+  TRYCUDA(cudaMemset(d.error_flag, 0, sizeof(unsigned)), "clear error flag");
+  {
+    int khz = 0;
+    cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, cfg->device);
+    // Every device-side wait gives up after about two seconds.
+    d.timeout_cycles = (long long)(khz > 0 ? khz : 2000000) * 1000LL * 2;
+  }
+  d.pipeline = cfg->kernel != LBMC_KERNEL_DIRECT;
+  TRYCUDA(h->ops->plan(d), "kernel planning");
+  if (cfg->kernel == LBMC_KERNEL_PIPELINED && !d.use_pipeline) {
+    release(h);
+    return fail(LBMC_ERR_UNSUPPORTED,
+                "the bulk-copy pipeline needs Lx * element size to be a multiple of 16 bytes "
+                "and two stages of Q rows to fit in shared memory");
+  }
+  h->nblocks = d.nblocks;
   TRY(dev_alloc(h, &d.partials, sizeof(double) * DIAG_VALUES * h->nblocks, "diagnostic partials"));
   TRY(dev_alloc(h, &d.flag, sizeof(unsigned), "diagnostic flag"));
   TRY(dev_alloc(h, &h->diag_out, sizeof(double) * DIAG_VALUES, "diagnostics"));
@@ -529,6 +547,10 @@ extern "C" lbmc_status lbmc_iterate(lbmc_handle *h, int nsteps, unsigned flags) 
   }
   if (flags & LBMC_SYNC) {
     CK(cudaStreamSynchronize(h->stream), "lbmc_iterate");
+    unsigned err = 0;
+    CK(cudaMemcpy(&err, h->ds.error_flag, sizeof(err), cudaMemcpyDeviceToHost), "read error flag");
+    if (err & ERROR_TIMEOUT)
+      return fail(LBMC_ERR_TIMEOUT, "a device-side wait expired (bulk-copy pipeline)");
     if ((flags & LBMC_REDUCE_DIAG) && nsteps > 0) {
       unsigned flag = 0;
       CK(cudaMemcpy(&flag, h->ds.flag, sizeof(flag), cudaMemcpyDeviceToHost), "read flag");

@@ -33,6 +33,13 @@ struct DeviceState {
   int forcing;
   int blend;  // Noble-Torczynski partial nodes present
   uint16_t table[256];
+  unsigned *error_flag;     // device word, ERROR_TIMEOUT on an expired wait
+  long long timeout_cycles; // bound of every device-side wait
+  int pipeline;             // allow the bulk-copy pipelined kernel
+  int use_pipeline;         // chosen by plan()
+  int stages;               // shared-memory stages of the pipelined kernel
+  long long pipe_grid;      // persistent blocks of the pipelined kernel
+  long long nblocks;        // blocks of the step kernel (diagnostic partials)
 };
 
 struct LatticeStorageOps {
@@ -46,8 +53,8 @@ struct LatticeStorageOps {
   // Sets population i from natural-layout FP64 values at step counter t.
   cudaError_t (*upload_population)(const DeviceState &, long long t, int i, const double *in,
                                    cudaStream_t);
-  // Number of blocks the step kernel launches (diagnostic partial count).
-  long long (*step_blocks)(const DeviceState &);
+  // Chooses the step kernel and launch geometry; sets nblocks.
+  cudaError_t (*plan)(DeviceState &);
 };
 
 const LatticeStorageOps *ops_d2q9_f32();

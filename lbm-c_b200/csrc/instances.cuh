@@ -37,6 +37,10 @@ struct Launchers {
     a.inv_scale = (C)(1.0 / d.scale);
     a.compat = d.compat;
     a.store = store ? 1 : 0;
+    a.error_flag = d.error_flag;
+    a.timeout_cycles = d.timeout_cycles;
+    a.rows = (long long)d.L[1] * d.L[2];
+    a.stages = d.stages;
     for (int k = 0; k < 256; k++) a.table[k] = d.table[k];
     return a;
   }
@@ -55,26 +59,54 @@ struct Launchers {
     return (long long)g.x * g.y * g.z;
   }
 
+  // Pipelined (bulk-copy) launch geometry: stages of Q rows in shared memory.
+  static size_t stage_bytes(const DeviceState &d) { return (size_t)L::Q * d.L[0] * sizeof(S); }
+  static bool pipelined_eligible(const DeviceState &d) {
+    return d.pipeline && (d.L[0] * sizeof(S)) % 16 == 0 && 2 * stage_bytes(d) <= 200 * 1024;
+  }
+  static int pipe_stages(const DeviceState &d) {
+    long long st = (64 * 1024) / (long long)stage_bytes(d);
+    if (st < 2) st = 2;
+    if (st > PIPE_MAX_STAGES) st = PIPE_MAX_STAGES;
+    return (int)st;
+  }
+  static int pipe_threads(const DeviceState &d) {
+    int bx = (d.L[0] + 31) / 32 * 32;
+    return bx < STEP_BLOCK ? bx : STEP_BLOCK;
+  }
+
   template <int COL, bool FORCE, bool BLEND, bool DIAG>
-  static void launch(const StepArgs<C> &a, const DeviceState &d, cudaStream_t st) {
-    step_kernel<L, S, COL, FORCE, BLEND, DIAG><<<grid_dim(d), block_dim(d), 0, st>>>(a);
+  static cudaError_t launch(const StepArgs<C> &a, const DeviceState &d, cudaStream_t st) {
+    if (d.use_pipeline) {
+      auto kern = step_pipelined_kernel<L, S, COL, FORCE, BLEND, DIAG>;
+      const size_t smem = (size_t)d.stages * stage_bytes(d);
+      static thread_local size_t configured = 0;  // per instantiation
+      if (configured < smem) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = smem;
+      }
+      kern<<<(unsigned)d.pipe_grid, pipe_threads(d), smem, st>>>(a);
+    } else {
+      step_kernel<L, S, COL, FORCE, BLEND, DIAG><<<grid_dim(d), block_dim(d), 0, st>>>(a);
+    }
+    return cudaSuccess;
   }
 
   template <int COL, bool BLEND>
-  static void launch_fd(const StepArgs<C> &a, const DeviceState &d, bool diag, cudaStream_t st) {
+  static cudaError_t launch_fd(const StepArgs<C> &a, const DeviceState &d, bool diag, cudaStream_t st) {
     if (d.forcing) {
-      if (diag) launch<COL, true, BLEND, true>(a, d, st);
-      else launch<COL, true, BLEND, false>(a, d, st);
-    } else {
-      if (diag) launch<COL, false, BLEND, true>(a, d, st);
-      else launch<COL, false, BLEND, false>(a, d, st);
+      if (diag) return launch<COL, true, BLEND, true>(a, d, st);
+      return launch<COL, true, BLEND, false>(a, d, st);
     }
+    if (diag) return launch<COL, false, BLEND, true>(a, d, st);
+    return launch<COL, false, BLEND, false>(a, d, st);
   }
 
   template <int COL>
-  static void launch_col(const StepArgs<C> &a, const DeviceState &d, bool diag, cudaStream_t st) {
-    if (d.blend) launch_fd<COL, true>(a, d, diag, st);
-    else launch_fd<COL, false>(a, d, diag, st);
+  static cudaError_t launch_col(const StepArgs<C> &a, const DeviceState &d, bool diag, cudaStream_t st) {
+    if (d.blend) return launch_fd<COL, true>(a, d, diag, st);
+    return launch_fd<COL, false>(a, d, diag, st);
   }
 
   static cudaError_t step(const DeviceState &d, long long t, bool store, bool diag,
@@ -85,12 +117,54 @@ struct Launchers {
       sf_gather_kernel<L, S><<<nb, 128, 0, st>>>(a, d.sf_nodes, d.sf_face, d.n_sf,
                                                   static_cast<C *>(d.sf_buf));
     }
+    cudaError_t e;
     switch (d.col) {
-      case COL_BGK: launch_col<COL_BGK>(a, d, diag, st); break;
-      case COL_BGK_SMAG: launch_col<COL_BGK_SMAG>(a, d, diag, st); break;
-      default: launch_col<COL_MRT>(a, d, diag, st); break;
+      case COL_BGK: e = launch_col<COL_BGK>(a, d, diag, st); break;
+      case COL_BGK_SMAG: e = launch_col<COL_BGK_SMAG>(a, d, diag, st); break;
+      default: e = launch_col<COL_MRT>(a, d, diag, st); break;
     }
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
+  }
+
+  // Chooses the kernel and its launch geometry for a handle (called once by
+  // lbmc_init after the device state is filled in).
+  static cudaError_t plan(DeviceState &d) {
+    d.use_pipeline = pipelined_eligible(d) ? 1 : 0;
+    if (!d.use_pipeline) {
+      d.nblocks = blocks(d);
+      return cudaSuccess;
+    }
+    d.stages = pipe_stages(d);
+    const size_t smem = (size_t)d.stages * stage_bytes(d);
+    // Occupancy of the heaviest instantiation the handle can launch.
+    int per_sm = 0;
+    cudaError_t e;
+    auto probe = [&](auto kern) {
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pipe_threads(d), smem);
+    };
+    switch (d.col) {
+      case COL_BGK: probe(step_pipelined_kernel<L, S, COL_BGK, true, true, true>); break;
+      case COL_BGK_SMAG: probe(step_pipelined_kernel<L, S, COL_BGK_SMAG, true, true, true>); break;
+      default: probe(step_pipelined_kernel<L, S, COL_MRT, true, true, true>); break;
+    }
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) {
+      d.use_pipeline = 0;
+      d.nblocks = blocks(d);
+      return cudaSuccess;
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long rows = (long long)d.L[1] * d.L[2];
+    long long grid = (long long)sms * per_sm;
+    if (grid > rows) grid = rows;
+    d.pipe_grid = grid;
+    d.nblocks = grid;
+    return cudaSuccess;
   }
 
   static cudaError_t fetch_population(const DeviceState &d, long long t, int i, double *out,
@@ -109,7 +183,7 @@ struct Launchers {
 
   static const LatticeStorageOps *ops() {
     static const LatticeStorageOps o = {(int)sizeof(C), (int)sizeof(S), &step, &fetch_population,
-                                        &upload_population, &blocks};
+                                        &upload_population, &plan};
     return &o;
   }
 };

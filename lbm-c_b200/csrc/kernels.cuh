@@ -119,8 +119,14 @@ struct StepArgs {
   C scale, inv_scale;
   unsigned compat;
   int store;
+  unsigned *error_flag;         // bit 0: a bounded device wait expired
+  long long timeout_cycles;     // limit of every device-side wait
+  long long rows;               // Ly * Lz (pipelined kernel)
+  int stages;                   // shared-memory stages (pipelined kernel)
   uint16_t table[256];
 };
+
+constexpr unsigned ERROR_TIMEOUT = 1u;
 
 // ----------------------------------------------------------- index helpers
 
@@ -172,21 +178,33 @@ struct Node {
 };
 
 template <class L>
-__device__ __forceinline__ constexpr double weight(int i) {
+__host__ __device__ constexpr double weight(int i) {
   return (double)L::wn(i) / (double)L::wd;
+}
+
+// e_I . v for a compile-time population I.
+template <class L, int I, class C>
+__device__ __forceinline__ C edot(const C *v) {
+  C r = 0;
+  if constexpr (L::e(0, I) != 0) r += C(L::e(0, I)) * v[0];
+  if constexpr (L::e(1, I) != 0) r += C(L::e(1, I)) * v[1];
+  if constexpr (L::DIM > 2 && L::e(2, I) != 0) r += C(L::e(2, I)) * v[2];
+  return r;
 }
 
 // rho = 1 + sum g, u = sum e g / rho (LBM-C/solver.cu:96-108).
 template <class L, class C>
 __device__ __forceinline__ void moments(Node<L, C> &nd) {
-  C d = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-  for (int i = 0; i < L::Q; i++) {
-    d += nd.g[i];
-    if (L::e(0, i)) jx += L::e(0, i) * nd.g[i];
-    if (L::e(1, i)) jy += L::e(1, i) * nd.g[i];
-    if (L::DIM > 2 && L::e(2, i)) jz += L::e(2, i) * nd.g[i];
-  }
+  C d = nd.g[0], jx = 0, jy = 0, jz = 0;
+  unroll<L::NP>([&](auto pc) {
+    constexpr int i = L::pair(decltype(pc)::value);
+    constexpr int o = L::opp(i);
+    const C sum = nd.g[i] + nd.g[o], dif = nd.g[i] - nd.g[o];
+    d += sum;
+    if constexpr (L::e(0, i) != 0) jx += C(L::e(0, i)) * dif;
+    if constexpr (L::e(1, i) != 0) jy += C(L::e(1, i)) * dif;
+    if constexpr (L::DIM > 2 && L::e(2, i) != 0) jz += C(L::e(2, i)) * dif;
+  });
   nd.drho = d;
   nd.rho = C(1) + d;
   const C inv = C(1) / nd.rho;
@@ -360,64 +378,14 @@ __device__ __forceinline__ void apply_micro(Node<L, C> &nd, int code, const Step
     return;
   }
   const C *row = a.sf_buf + (long long)a.sf_index[n] * L::Q;
-#pragma unroll
-  for (int i = 0; i < L::Q; i++) {
-#pragma unroll
-    for (int fc = 0; fc < 2 * L::DIM; fc++)
-      if (fc == face && sf_unknown<L>(fc, i)) nd.g[i] = row[i];
-  }
-}
-
-// e_i . v for a compile-time population i.
-template <class L, class C>
-__device__ __forceinline__ C edot(int i, const C *v) {
-  C r = 0;
-  if (L::e(0, i)) r += C(L::e(0, i)) * v[0];
-  if (L::e(1, i)) r += C(L::e(1, i)) * v[1];
-  if (L::DIM > 2 && L::e(2, i)) r += C(L::e(2, i)) * v[2];
-  return r;
-}
-
-// Equilibrium deviation geq_i = f_eq_i - w_i = w_i (drho + rho (eu + eu^2/2 - usq))
-// with eu = 3 e.u and usq = 1.5 u.u (LBM-C/collision.cu:53-59).
-template <class L, class C>
-__device__ __forceinline__ C geq_dev(int i, const Node<L, C> &nd, C usq) {
-  const C eu = C(3) * edot<L>(i, nd.u);
-  return C(weight<L>(i)) * (nd.drho + nd.rho * (eu + C(0.5) * eu * eu - usq));
-}
-
-// Guo source (LBM-C/collision.cu:82-99), after u <- u + F/(2 rho):
-// F_i = w_i (1 - 1/(2 tau)) [3 (e_i - u) + 9 (e_i.u) e_i] . F
-//     = w_i pre (3 (e_i.F - u.F) + 9 (e_i.u)(e_i.F)).
-template <class L, class C>
-__device__ __forceinline__ C guo_term(int i, const Node<L, C> &nd, const C *F, C pre, C uF) {
-  const C eF = edot<L>(i, F);
-  const C eu = edot<L>(i, nd.u);
-  return C(weight<L>(i)) * pre * (C(3) * (eF - uF) + C(9) * eu * eF);
-}
-
-// Smagorinsky relaxation time (LBM-C/collision.cu:445-463, q_bar zeroed):
-// q_ab = sum_i e_a e_b (f - f_eq), q_hat = sum_ab sqrt(2 q_ab^2),
-// tau_eff = tau + (sqrt(tau^2 + 2 sqrt2 C^2 (9/rho) q_hat) - tau)/2.
-template <class L, class C>
-__device__ __forceinline__ C smagorinsky_tau(const Node<L, C> &nd, C usq, C tau, C cs) {
-  C q[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, yz, xz
-#pragma unroll
-  for (int i = 0; i < L::Q; i++) {
-    const C neq = nd.g[i] - geq_dev<L>(i, nd, usq);
-    const int ex = L::e(0, i), ey = L::e(1, i), ez = L::e(2, i);
-    if (ex) q[0] += neq;
-    if (ey) q[1] += neq;
-    if (ez) q[2] += neq;
-    if (ex * ey) q[3] += C(ex * ey) * neq;
-    if (ey * ez) q[4] += C(ey * ez) * neq;
-    if (ex * ez) q[5] += C(ex * ez) * neq;
-  }
-  const C r2 = sqrt(C(2));
-  C qhat = r2 * (fabs(q[0]) + fabs(q[1]) + C(2) * fabs(q[3]));
-  if (L::DIM > 2) qhat += r2 * (fabs(q[2]) + C(2) * (fabs(q[4]) + fabs(q[5])));
-  const C k = C(2) * r2 * cs * cs * (C(9) / nd.rho);
-  return tau + C(0.5) * (sqrt(tau * tau + k * qhat) - tau);
+  unroll<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    bool take = false;
+    unroll<2 * L::DIM>([&](auto fc) {
+      if constexpr (sf_unknown<L>(decltype(fc)::value, i)) take |= (face == decltype(fc)::value);
+    });
+    if (take) nd.g[i] = row[i];
+  });
 }
 
 // k-th MRT moment-equilibrium deviation meq_k - (M w)_k
@@ -461,8 +429,233 @@ __device__ __forceinline__ C meq_dev(int k, const Node<L, C> &nd, unsigned compa
   }
 }
 
+// The fluid-node collision of the reference (collision_functions[2 type +
+// forcing], LBM-C/collision.cu:19-421) after the macro/micro BCs
+// (LBM-C/solver.cu:111-112), written with opposite-pair symmetry: for a pair
+// (i, o = opp(i)), e_o = -e_i and w_o = w_i, so the equilibria, Guo terms
+// and the MRT transforms split into even and odd parts computed once per
+// pair.  Post-collision deviations go to out[].
+template <class L, class C, int COL, bool FORCE, bool BLEND>
+__device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> &a, int n,
+                                              unsigned entry, C (&out)[L::Q]) {
+  constexpr int Q = L::Q;
+  C B = 0;
+  if (entry) {
+    const int macro = entry & ENTRY_MACRO_MASK;
+    const int micro = (entry & ENTRY_MICRO_MASK) >> ENTRY_MICRO_SHIFT;
+    if (macro) apply_macro(nd, macro, a, n);
+    if (micro) apply_micro(nd, micro, a, n);
+    if (BLEND && (entry & ENTRY_PARTIAL)) B = a.B[n];
+  }
+  const C tau0 = a.tau;
+  C F[3] = {0, 0, 0}, pre = 0, uF = 0;
+  if constexpr (FORCE) {
+    if (a.force[0]) {
+      F[0] = a.force[0][n];
+      F[1] = a.force[1][n];
+      if (L::DIM > 2) F[2] = a.force[2][n];
+    } else {
+      F[0] = a.force_u[0];
+      F[1] = a.force_u[1];
+      F[2] = a.force_u[2];
+    }
+    // u <- u + F/(2 rho) (collision.cu:74-78)
+    const C h = C(1) / (C(2) * nd.rho);
+    nd.u[0] += h * F[0];
+    nd.u[1] += h * F[1];
+    if (L::DIM > 2) nd.u[2] += h * F[2];
+    pre = C(1) - C(1) / (C(2) * tau0);
+    uF = nd.u[0] * F[0] + nd.u[1] * F[1] + (L::DIM > 2 ? nd.u[2] * F[2] : C(0));
+  }
+  const C omb = C(1) - B;
+  // Guo source (collision.cu:82-99): F_i = w_i pre (3 (e_i.F - u.F) + 9 (e_i.u)(e_i.F)),
+  // even part w pre (9 (e.u)(e.F) - 3 u.F), odd part 3 w pre e.F.
+  auto guo_parts = [&](auto ic, C &even, C &odd) {
+    if constexpr (FORCE) {
+      constexpr int i = decltype(ic)::value;
+      const C wp = C(weight<L>(i)) * pre;
+      const C eF = edot<L, i>(F), eu = edot<L, i>(nd.u);
+      even = wp * (C(9) * eu * eF - C(3) * uF);
+      odd = wp * C(3) * eF;
+    } else {
+      even = 0;
+      odd = 0;
+    }
+  };
+  C ft0e, ft0o;
+  guo_parts(std::integral_constant<int, 0>{}, ft0e, ft0o);
+
+  if constexpr (COL == COL_MRT) {
+    // m* = S (M g - meq) / D; f <- f - M^T m* (collision.cu:192-303)
+    C S[L::NP], D[L::NP];
+    unroll<L::NP>([&](auto pc) {
+      constexpr int p = decltype(pc)::value;
+      constexpr int i = L::pair(p);
+      S[p] = nd.g[i] + nd.g[L::opp(i)];
+      D[p] = nd.g[i] - nd.g[L::opp(i)];
+    });
+    C ms[Q];
+    unroll<Q>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      constexpr bool even = moment_even<L>(k);
+      C mk = 0;
+      if constexpr (even && L::m(k, 0) != 0) mk = C(L::m(k, 0)) * nd.g[0];
+      unroll<L::NP>([&](auto pc) {
+        constexpr int p = decltype(pc)::value;
+        constexpr int c = L::m(k, L::pair(p));
+        const C v = even ? S[p] : D[p];
+        if constexpr (c == 1) mk += v;
+        else if constexpr (c == -1) mk -= v;
+        else if constexpr (c != 0) mk += C(c) * v;
+      });
+      constexpr double inv_norm = 1.0 / (double)L::mnorm(k);
+      ms[k] = a.s_mrt[k] * (mk - meq_dev<L>(k, nd, a.compat)) * C(inv_norm);
+    });
+    if (Q == 15 && (a.compat & COMPAT_D3Q15_MINV_ZERO)) {
+      // macros.cu:97-115: the reference's D3Q15 M_inv is all zeros.
+      unroll<Q>([&](auto kc) { ms[decltype(kc)::value] = 0; });
+    }
+    // population 0
+    {
+      C acc = 0;
+      unroll<Q>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        constexpr int c = L::m(k, 0);
+        if constexpr (c != 0) acc += C(c) * ms[k];
+      });
+      out[0] = nd.g[0] - omb * acc + omb * ft0e;
+    }
+    const bool inplace = BLEND && (a.compat & COMPAT_MRTPOR_INPLACE);
+    unroll<L::NP>([&](auto pc) {
+      constexpr int i = L::pair(decltype(pc)::value);
+      constexpr int o = L::opp(i);
+      C E = 0, O = 0;
+      unroll<Q>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        constexpr int c = L::m(k, i);
+        if constexpr (c != 0) {
+          if constexpr (moment_even<L>(k)) {
+            if constexpr (c == 1) E += ms[k];
+            else if constexpr (c == -1) E -= ms[k];
+            else E += C(c) * ms[k];
+          } else {
+            if constexpr (c == 1) O += ms[k];
+            else if constexpr (c == -1) O -= ms[k];
+            else O += C(c) * ms[k];
+          }
+        }
+      });
+      C fe, fo_;
+      guo_parts(std::integral_constant<int, i>{}, fe, fo_);
+      const C acc_i = E + O, acc_o = E - O;
+      const C ft_i = fe + fo_, ft_o = fe - fo_;
+      if constexpr (BLEND) {
+        // mrt_ntpor(_guo)_collision (collision.cu:305-421).  The reference
+        // loops i upwards and reads f[opp[i]] after the lower index of the
+        // pair was updated (collision.cu:340,416); COMPAT_MRTPOR_INPLACE
+        // reproduces that.
+        const C oi = nd.g[i] - omb * acc_i + omb * ft_i + B * (nd.g[o] - nd.g[i]);
+        const C partner = inplace ? oi : nd.g[i];
+        out[i] = oi;
+        out[o] = nd.g[o] - omb * acc_o + omb * ft_o + B * (partner - nd.g[o]);
+      } else {
+        out[i] = nd.g[i] - acc_i + ft_i;
+        out[o] = nd.g[o] - acc_o + ft_o;
+      }
+    });
+  } else {
+    // BGK family (collision.cu:49-190): geq_i = A + Bq, geq_o = A - Bq with
+    // A = w (drho + rho (eu^2/2 - usq)), Bq = w rho eu, eu = 3 e_i.u.
+    const C usq = C(1.5) * (nd.u[0] * nd.u[0] + nd.u[1] * nd.u[1] + nd.u[2] * nd.u[2]);
+    const C A0 = C(weight<L>(0)) * (nd.drho - nd.rho * usq);
+    C tau = tau0;
+    if constexpr (COL == COL_BGK_SMAG) {
+      // Smagorinsky (collision.cu:445-463, q_bar zeroed): q_ab = sum e_a e_b
+      // (f - f_eq) is even in e, so each pair contributes e_a e_b (S - 2A).
+      C q[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, yz, xz
+      unroll<L::NP>([&](auto pc) {
+        constexpr int i = L::pair(decltype(pc)::value);
+        const C eu = C(3) * edot<L, i>(nd.u);
+        const C A = C(weight<L>(i)) * (nd.drho + nd.rho * (C(0.5) * eu * eu - usq));
+        const C neq = nd.g[i] + nd.g[L::opp(i)] - C(2) * A;
+        constexpr int ex = L::e(0, i), ey = L::e(1, i), ez = L::e(2, i);
+        if constexpr (ex != 0) q[0] += neq;
+        if constexpr (ey != 0) q[1] += neq;
+        if constexpr (ez != 0) q[2] += neq;
+        if constexpr (ex * ey != 0) q[3] += C(ex * ey) * neq;
+        if constexpr (ey * ez != 0) q[4] += C(ey * ez) * neq;
+        if constexpr (ex * ez != 0) q[5] += C(ex * ez) * neq;
+      });
+      const C r2 = sqrt(C(2));
+      C qhat = r2 * (fabs(q[0]) + fabs(q[1]) + C(2) * fabs(q[3]));
+      if (L::DIM > 2) qhat += r2 * (fabs(q[2]) + C(2) * (fabs(q[4]) + fabs(q[5])));
+      const C k = C(2) * r2 * a.c_smag * a.c_smag * (C(9) / nd.rho);
+      tau = tau0 + C(0.5) * (sqrt(tau0 * tau0 + k * qhat) - tau0);
+    }
+    const C om = C(1) / tau;
+    // population 0 (e = 0)
+    out[0] = nd.g[0] - omb * (om * (nd.g[0] - A0)) + omb * ft0e;
+    unroll<L::NP>([&](auto pc) {
+      constexpr int i = L::pair(decltype(pc)::value);
+      constexpr int o = L::opp(i);
+      const C eu = C(3) * edot<L, i>(nd.u);
+      const C w = C(weight<L>(i));
+      const C A = w * (nd.drho + nd.rho * (C(0.5) * eu * eu - usq));
+      const C Bq = w * nd.rho * eu;
+      C fe, fo_;
+      guo_parts(std::integral_constant<int, i>{}, fe, fo_);
+      const C om_i = om * (nd.g[i] - (A + Bq));
+      const C om_o = om * (nd.g[o] - (A - Bq));
+      if constexpr (BLEND) {
+        // bgk_ntpor(_guo)_collision (collision.cu:113-190)
+        out[i] = nd.g[i] - omb * om_i + B * (nd.g[o] - nd.g[i]) + omb * (fe + fo_);
+        out[o] = nd.g[o] - omb * om_o + B * (nd.g[i] - nd.g[o]) + omb * (fe - fo_);
+      } else {
+        out[i] = nd.g[i] - om_i + (fe + fo_);
+        out[o] = nd.g[o] - om_o + (fe - fo_);
+      }
+    });
+  }
+}
+
+// bounceback (LBM-C/collision.cu:423-443): f_i <- f_opp(i), rho = u = 0.
+template <class L, class C>
+__device__ __forceinline__ void collide_solid(Node<L, C> &nd, C (&out)[L::Q]) {
+  unroll<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    out[i] = nd.g[L::opp(i)];
+  });
+  nd.drho = C(-1);
+  nd.rho = 0;
+  nd.u[0] = nd.u[1] = nd.u[2] = 0;
+}
+
+template <class L, class C>
+__device__ __forceinline__ void store_and_reduce(const Node<L, C> &nd, const StepArgs<C> &a, int n,
+                                                 double (&dv)[DIAG_VALUES], bool &nonfinite,
+                                                 bool diag) {
+  if (a.store) {
+    a.rho[n] = nd.drho;
+    a.u[0][n] = nd.u[0];
+    a.u[1][n] = nd.u[1];
+    if (L::DIM > 2) a.u[2][n] = nd.u[2];
+  }
+  if (diag) {
+    const double rho = (double)nd.drho + 1.0;
+    const double ux = nd.u[0], uy = nd.u[1], uz = nd.u[2];
+    dv[0] += rho;
+    dv[1] += rho * ux;
+    dv[2] += rho * uy;
+    dv[3] += rho * uz;
+    dv[4] += 0.5 * rho * (ux * ux + uy * uy + uz * uz);
+    nonfinite |= !(isfinite(rho) && isfinite(ux) && isfinite(uy) && isfinite(uz));
+  }
+}
+
 // ------------------------------------------------------------ diagnostics
 
+// Warp-shuffle + shared-memory block reduction of the FP64 sums; one partial
+// per block, summed in a fixed order by diag_finalize_kernel.
 template <class C>
 __device__ __forceinline__ void block_diag(const double (&v)[DIAG_VALUES], bool nonfinite,
                                            const StepArgs<C> &a, long long block) {
@@ -490,11 +683,11 @@ __device__ __forceinline__ void block_diag(const double (&v)[DIAG_VALUES], bool 
   }
 }
 
-// -------------------------------------------------------------- the step
+// ------------------------------------------------- direct-load step kernel
 
+// Fallback for rows whose byte length is not a multiple of 16 (bulk copies
+// need 16-byte granules) or that do not fit the shared-memory stages.
 // Grid: blockDim (bx, 1, 1) along x, gridDim (ceil(Lx/bx), Ly, Lz).
-// COL: COL_BGK / COL_BGK_SMAG / COL_MRT.  BLEND: Noble-Torczynski partial
-// solid nodes present (ColType NTPOR/MRTPOR).  DIAG: emit FP64 partial sums.
 template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG>
 __global__ void __launch_bounds__(STEP_BLOCK)
     step_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a) {
@@ -511,136 +704,231 @@ __global__ void __launch_bounds__(STEP_BLOCK)
     const int n = x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z);
     S *f = reinterpret_cast<S *>(a.f);
     Node<L, C> nd;
-#pragma unroll
-    for (int i = 0; i < Q; i++)
+    unroll<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
       nd.g[i] = Storage<S>::get(f + i * a.pitch + st.template slot<L>(i)) * a.inv_scale;
+    });
     const int cls = a.cls[n];
+    C out[Q];
     if (cls == CLASS_SOLID) {
-      // bounceback (LBM-C/collision.cu:423-443): f_i <- f_opp(i), rho = u = 0.
-#pragma unroll
-      for (int i = 0; i < Q; i++)
-        Storage<S>::put(f + i * a.pitch + st.template slot<L>(i), nd.g[L::opp(i)] * a.scale);
-      nd.drho = C(-1);
-      nd.rho = 0;
-      nd.u[0] = nd.u[1] = nd.u[2] = 0;
+      collide_solid(nd, out);
     } else {
       moments(nd);
-      const unsigned entry = cls ? a.table[cls] : 0u;
-      C B = 0;
-      if (entry) {
-        const int macro = entry & ENTRY_MACRO_MASK;
-        const int micro = (entry & ENTRY_MICRO_MASK) >> ENTRY_MICRO_SHIFT;
-        if (macro) apply_macro(nd, macro, a, n);
-        if (micro) apply_micro(nd, micro, a, n);
-        if (BLEND && (entry & ENTRY_PARTIAL)) B = a.B[n];
-      }
-      const C tau0 = a.tau;
-      C F[3] = {0, 0, 0}, pre = 0, uF = 0;
-      if (FORCE) {
-        if (a.force[0]) {
-          F[0] = a.force[0][n];
-          F[1] = a.force[1][n];
-          if (L::DIM > 2) F[2] = a.force[2][n];
-        } else {
-          F[0] = a.force_u[0];
-          F[1] = a.force_u[1];
-          F[2] = a.force_u[2];
-        }
-        // u <- u + F/(2 rho) (collision.cu:74-78)
-        const C h = C(1) / (C(2) * nd.rho);
-        nd.u[0] += h * F[0];
-        nd.u[1] += h * F[1];
-        if (L::DIM > 2) nd.u[2] += h * F[2];
-        pre = C(1) - C(1) / (C(2) * tau0);
-        uF = nd.u[0] * F[0] + nd.u[1] * F[1] + (L::DIM > 2 ? nd.u[2] * F[2] : C(0));
-      }
-      const C omb = C(1) - B;
-      if (COL == COL_MRT) {
-        // m* = S (M g - meq) / D; f <- f - M^T m* (collision.cu:192-303)
-        C ms[Q];
-        unroll<Q>([&](auto kc) {
-          constexpr int k = decltype(kc)::value;
-          C mk = 0;
-          unroll<Q>([&](auto ic) {
-            constexpr int i = decltype(ic)::value;
-            constexpr int mki = L::m(k, i);
-            if constexpr (mki == 1) mk += nd.g[i];
-            else if constexpr (mki == -1) mk -= nd.g[i];
-            else if constexpr (mki != 0) mk += C(mki) * nd.g[i];
-          });
-          constexpr double inv_norm = 1.0 / (double)L::mnorm(k);
-          ms[k] = a.s_mrt[k] * (mk - meq_dev<L>(k, nd, a.compat)) * C(inv_norm);
-        });
-        const bool minv_zero = Q == 15 && (a.compat & COMPAT_D3Q15_MINV_ZERO);
-        const bool inplace = BLEND && (a.compat & COMPAT_MRTPOR_INPLACE);
-        C keep[Q] = {};
-        unroll<Q>([&](auto ic) {
-          constexpr int i = decltype(ic)::value;
-          constexpr int o = L::opp(i);
-          C acc = 0;
-          unroll<Q>([&](auto kc) {
-            constexpr int k = decltype(kc)::value;
-            constexpr int mki = L::m(k, i);
-            if constexpr (mki == 1) acc += ms[k];
-            else if constexpr (mki == -1) acc -= ms[k];
-            else if constexpr (mki != 0) acc += C(mki) * ms[k];
-          });
-          if (minv_zero) acc = 0;
-          const C ft = FORCE ? guo_term<L>(i, nd, F, pre, uF) : C(0);
-          C out;
-          if constexpr (BLEND) {
-            // mrt_ntpor(_guo)_collision (collision.cu:305-421).  The reference
-            // reads f[opp[i]] after lower indices were already updated
-            // (collision.cu:340,416); COMPAT_MRTPOR_INPLACE reproduces that.
-            C fo = nd.g[o];
-            if constexpr (o < i) {
-              if (inplace) fo = keep[o];
-            }
-            out = nd.g[i] - omb * acc + omb * ft + B * (fo - nd.g[i]);
-            keep[i] = out;
-          } else {
-            out = nd.g[i] - acc + ft;
-          }
-          Storage<S>::put(f + i * a.pitch + st.template slot<L>(i), out * a.scale);
-        });
-      } else {
-        const C usq = C(1.5) * (nd.u[0] * nd.u[0] + nd.u[1] * nd.u[1] + nd.u[2] * nd.u[2]);
-        C tau = tau0;
-        if (COL == COL_BGK_SMAG) tau = smagorinsky_tau(nd, usq, tau0, a.c_smag);
-        const C om = C(1) / tau;
-#pragma unroll
-        for (int i = 0; i < Q; i++) {
-          const C omega_i = om * (nd.g[i] - geq_dev<L>(i, nd, usq));
-          const C ft = FORCE ? guo_term<L>(i, nd, F, pre, uF) : C(0);
-          C out;
-          if (BLEND)  // bgk_ntpor(_guo)_collision (collision.cu:113-190)
-            out = nd.g[i] - omb * omega_i + B * (nd.g[L::opp(i)] - nd.g[i]) + omb * ft;
-          else
-            out = nd.g[i] - omega_i + ft;
-          Storage<S>::put(f + i * a.pitch + st.template slot<L>(i), out * a.scale);
-        }
-      }
+      collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
     }
-    if (a.store) {
-      a.rho[n] = nd.drho;
-      a.u[0][n] = nd.u[0];
-      a.u[1][n] = nd.u[1];
-      if (L::DIM > 2) a.u[2][n] = nd.u[2];
-    }
-    if (DIAG) {
-      const double rho = (double)nd.drho + 1.0;
-      const double ux = nd.u[0], uy = nd.u[1], uz = nd.u[2];
-      dv[0] = rho;
-      dv[1] = rho * ux;
-      dv[2] = rho * uy;
-      dv[3] = rho * uz;
-      dv[4] = 0.5 * rho * (ux * ux + uy * uy + uz * uz);
-      nonfinite = !(isfinite(rho) && isfinite(ux) && isfinite(uy) && isfinite(uz));
-    }
+    unroll<Q>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      Storage<S>::put(f + i * a.pitch + st.template slot<L>(i), out[i] * a.scale);
+    });
+    store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
   }
   if (DIAG)
     block_diag<C>(dv, nonfinite, a,
                   blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z));
+}
+
+// -------------------------------------------- bulk-copy pipelined kernel
+
+// Shared-memory staging of whole population rows with cp.async.bulk (the
+// TMA engine's 1-D bulk copies) and mbarrier completion.  For the shift
+// layout, the nodes of one grid row (y, z) read population i from one whole
+// physical row, (y - t e_y, z - t e_z) rotated by t e_x along x, and write
+// their results back to the same slots; so a row is: bulk-load Q rows,
+// collide every node from shared memory, bulk-store the Q rows.  The
+// persistent blocks walk rows r = blockIdx.x, blockIdx.x + gridDim.x, ...
+// with `stages` rows in flight, so memory traffic is decoupled from the
+// compute of the current row.  No cluster multicast is used.
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after `limit` cycles and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, long long limit) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > limit) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_store(void *dst, unsigned src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Global address of population i's physical row for grid row (y, z).
+template <class L, class S>
+__device__ __forceinline__ S *phys_row(S *f, long long pitch, int i, int y, int z, const int *s,
+                                       const int *L_) {
+  int yy = y, zz = z;
+  const int ey = L::e(1, i), ez = L::e(2, i);
+  if (ey > 0) yy = wrap_sub(y, s[1], L_[1]);
+  if (ey < 0) yy = wrap_add(y, s[1], L_[1]);
+  if (ez > 0) zz = wrap_sub(z, s[2], L_[2]);
+  if (ez < 0) zz = wrap_add(z, s[2], L_[2]);
+  return f + i * pitch + (long long)L_[0] * (yy + (long long)L_[1] * zz);
+}
+
+template <class L, class S>
+__device__ __forceinline__ void issue_row_load(S *f, long long pitch, long long row, const int *s,
+                                               const int *L_, S *stage_buf, unsigned bar) {
+  const int y = (int)(row % L_[1]), z = (int)(row / L_[1]);
+  const unsigned bytes = (unsigned)(L_[0] * sizeof(S));
+  mbar_expect_tx(bar, bytes * L::Q);
+#pragma unroll
+  for (int i = 0; i < L::Q; i++)
+    bulk_load(smem_addr(stage_buf + (long long)i * L_[0]), phys_row<L>(f, pitch, i, y, z, s, L_), bytes,
+              bar);
+}
+
+template <class L, class S>
+__device__ __forceinline__ void issue_row_store(S *f, long long pitch, long long row, const int *s,
+                                                const int *L_, S *stage_buf) {
+  const int y = (int)(row % L_[1]), z = (int)(row / L_[1]);
+  const unsigned bytes = (unsigned)(L_[0] * sizeof(S));
+#pragma unroll
+  for (int i = 0; i < L::Q; i++)
+    bulk_store(phys_row<L>(f, pitch, i, y, z, s, L_), smem_addr(stage_buf + (long long)i * L_[0]), bytes);
+  bulk_commit();
+}
+
+constexpr int PIPE_MAX_STAGES = 8;
+
+// Dynamic shared memory: [stages][Q][Lx] storage elements.
+template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG>
+__global__ void __launch_bounds__(STEP_BLOCK)
+    step_pipelined_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a) {
+  using C = typename Storage<S>::C;
+  constexpr int Q = L::Q;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long full_bar[PIPE_MAX_STAGES];
+  __shared__ int abort_flag;
+  S *buf = reinterpret_cast<S *>(smem_raw);
+  const int lx = a.L[0];
+  const int nst = a.stages;
+  const long long stage_elems = (long long)Q * lx;
+  S *f = reinterpret_cast<S *>(a.f);
+  const long long rows = a.rows;
+  const long long my_rows = rows > blockIdx.x ? (rows - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const bool leader = threadIdx.x == 0;
+
+  if (leader) {
+    for (int k = 0; k < nst; k++) mbar_init(smem_addr(&full_bar[k]), 1);
+    mbar_fence_init();
+    abort_flag = 0;
+  }
+  __syncthreads();
+  if (leader) {
+    for (long long k = 0; k < nst - 1 && k < my_rows; k++)
+      issue_row_load<L>(f, a.pitch, blockIdx.x + k * gridDim.x, a.s, a.L, buf + (k % nst) * stage_elems,
+                        smem_addr(&full_bar[k % nst]));
+  }
+  // x positions of this thread's nodes along the row, and their shifted slots
+  double dv[DIAG_VALUES] = {0, 0, 0, 0, 0};
+  bool nonfinite = false;
+  long long k = 0;
+  for (; k < my_rows; k++) {
+    const int st_idx = (int)(k % nst);
+    const unsigned parity = (unsigned)((k / nst) & 1);
+    if (!mbar_wait_bounded(smem_addr(&full_bar[st_idx]), parity, a.timeout_cycles)) {
+      atomicOr(a.error_flag, ERROR_TIMEOUT);
+      abort_flag = 1;
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    const long long row = blockIdx.x + k * gridDim.x;
+    const int y = (int)(row % a.L[1]), z = (int)(row / a.L[1]);
+    S *sb = buf + st_idx * stage_elems;
+    for (int x = threadIdx.x; x < lx; x += blockDim.x) {
+      const int xp = wrap_sub(x, a.s[0], lx);  // e_x = +1 reads x - s
+      const int xm = wrap_add(x, a.s[0], lx);  // e_x = -1 reads x + s
+      const int n = x + lx * (y + a.L[1] * z);
+      Node<L, C> nd;
+      unroll<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        constexpr int ex = L::e(0, i);
+        const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
+        nd.g[i] = Storage<S>::get(sb + i * lx + xs) * a.inv_scale;
+      });
+      const int cls = a.cls[n];
+      C out[Q];
+      if (cls == CLASS_SOLID) {
+        collide_solid(nd, out);
+      } else {
+        moments(nd);
+        collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
+      }
+      unroll<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        constexpr int ex = L::e(0, i);
+        const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
+        Storage<S>::put(sb + i * lx + xs, out[i] * a.scale);
+      });
+      store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (leader) {
+      issue_row_store<L>(f, a.pitch, row, a.s, a.L, sb);
+      // The stage that held row k-1 is refilled with row k + nst - 1 once its
+      // store has finished reading shared memory.
+      const long long next = k + nst - 1;
+      if (next < my_rows) {
+        bulk_wait_read<1>();
+        const int ns = (int)(next % nst);
+        issue_row_load<L>(f, a.pitch, blockIdx.x + next * gridDim.x, a.s, a.L, buf + ns * stage_elems,
+                          smem_addr(&full_bar[ns]));
+      }
+    }
+  }
+  if (leader) {
+    bulk_wait_all();
+    if (abort_flag) {
+      // Drain loads that were issued but not consumed (bounded), so no copy
+      // still targets this block's shared memory when it exits.
+      for (long long j = k; j < my_rows && j < k + nst; j++) {
+        mbar_wait_bounded(smem_addr(&full_bar[j % nst]), (unsigned)((j / nst) & 1), a.timeout_cycles);
+      }
+    }
+  }
+  if (DIAG) block_diag<C>(dv, nonfinite, a, blockIdx.x);
 }
 
 // Stress-free pre-pass: before the step, copy the inward populations of each
@@ -667,19 +955,20 @@ __global__ void sf_gather_kernel(const __grid_constant__ StepArgs<typename Stora
   Sites st;
   st.init(c[0], c[1], c[2], a.s, a.L);
   const S *f = reinterpret_cast<const S *>(a.f);
-#pragma unroll
-  for (int i = 0; i < L::Q; i++) {
+  unroll<L::Q>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
     bool need = false;
-#pragma unroll
-    for (int fc = 0; fc < 2 * L::DIM; fc++) need |= (fc == face) && sf_unknown<L>(fc, i);
+    unroll<2 * L::DIM>([&](auto fc) {
+      if constexpr (sf_unknown<L>(decltype(fc)::value, i)) need |= (face == decltype(fc)::value);
+    });
     if (need)
       sf_buf[(long long)k * L::Q + i] =
           Storage<S>::get(f + i * a.pitch + st.template slot<L>(i)) * a.inv_scale;
-  }
+  });
 }
 
 // Natural-layout FP64 copy of population i: out[x] = w_i + g_i(x).
-// Grid as for the step kernel.
+// Grid as for the direct step kernel.
 template <class L, class S>
 __global__ void fetch_population_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a,
                                         int i, double *out) {
@@ -689,10 +978,11 @@ __global__ void fetch_population_kernel(const __grid_constant__ StepArgs<typenam
   st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
   const int n = x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z);
   const S *f = reinterpret_cast<const S *>(a.f);
-#pragma unroll
-  for (int k = 0; k < L::Q; k++)
+  unroll<L::Q>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
     if (k == i)
       out[n] = weight<L>(k) + (double)(Storage<S>::get(f + k * a.pitch + st.template slot<L>(k)) * a.inv_scale);
+  });
 }
 
 // Writes population i from natural-layout FP64 values into its slots for
@@ -707,10 +997,11 @@ __global__ void upload_population_kernel(const __grid_constant__ StepArgs<typena
   st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
   const int n = x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z);
   S *f = reinterpret_cast<S *>(a.f);
-#pragma unroll
-  for (int k = 0; k < L::Q; k++)
+  unroll<L::Q>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
     if (k == i)
       Storage<S>::put(f + k * a.pitch + st.template slot<L>(k), (C)(in[n] - weight<L>(k)) * a.scale);
+  });
 }
 
 }  // namespace lbmc

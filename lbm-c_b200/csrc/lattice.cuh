@@ -29,6 +29,12 @@ struct D2Q9 {
     constexpr int t[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
     return t[i];
   }
+  // Opposite pairs (i, opp(i)) with i < opp(i); population 0 is its own.
+  static constexpr int NP = 4;
+  __host__ __device__ static constexpr int pair(int p) {
+    constexpr int t[4] = {1, 2, 5, 6};
+    return t[p];
+  }
   // Weights as exact rationals w = wn / wd.
   __host__ __device__ static constexpr int wn(int i) { return i == 0 ? 16 : (i < 5 ? 4 : 1); }
   static constexpr int wd = 36;
@@ -66,6 +72,11 @@ struct D3Q15 {
     constexpr int t[15] = {0, 2, 1, 4, 3, 6, 5, 14, 13, 12, 11, 10, 9, 8, 7};
     return t[i];
   }
+  static constexpr int NP = 7;
+  __host__ __device__ static constexpr int pair(int p) {
+    constexpr int t[7] = {1, 3, 5, 7, 8, 9, 10};
+    return t[p];
+  }
   __host__ __device__ static constexpr int wn(int i) { return i == 0 ? 16 : (i < 7 ? 8 : 1); }
   static constexpr int wd = 72;
   __host__ __device__ static constexpr int c2(int i) {
@@ -97,5 +108,14 @@ struct D3Q15 {
     return s;
   }
 };
+
+// A moment row is even when it takes the same value on opposite populations
+// (rho, energy, stresses) and odd when it changes sign (momentum, fluxes).
+template <class L>
+__host__ __device__ constexpr bool moment_even(int k) {
+  for (int i = 0; i < L::Q; i++)
+    if (L::m(k, L::opp(i)) != L::m(k, i)) return false;
+  return true;
+}
 
 }  // namespace lbmc

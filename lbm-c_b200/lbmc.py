@@ -26,6 +26,7 @@ F32, F16, BF16, F64 = 0, 1, 2, 3
 BGK, NTPOR, MRT, MRTPOR = 0, 1, 2, 3
 INIT_STATIC, INIT_EQUILIBRIUM, INIT_F = 0, 1, 2
 STREAM_SHIFT, STREAM_AA = 0, 1
+KERNEL_AUTO, KERNEL_DIRECT, KERNEL_PIPELINED = 0, 1, 2
 COMPAT_D3Q15_MINV_ZERO = 1 << 0
 COMPAT_MEQ_INT_DIV = 1 << 1
 COMPAT_ZH_Z_UX = 1 << 2
@@ -52,7 +53,7 @@ class Config(ctypes.Structure):
                 ("storage", ctypes.c_int), ("streaming", ctypes.c_int),
                 ("compat", ctypes.c_uint), ("storage_scale", ctypes.c_double),
                 ("device", ctypes.c_int), ("block_size", ctypes.c_int),
-                ("reserved", ctypes.c_int * 6)]
+                ("kernel", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
 
 
 class Domain(ctypes.Structure):
@@ -100,6 +101,8 @@ def library() -> ctypes.CDLL:
         lib.lbmc_classify.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(Domain), _P, _P,
                                       ctypes.POINTER(ctypes.c_int)]
         lib.lbmc_lattice_tables.argtypes = [ctypes.c_int, _P, _P, _P, _P]
+        lib.lbmc_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_double]
+        lib.lbmc_selftest_wait_timeout.restype = ctypes.c_int
         for name in ("lbmc_config_default", "lbmc_validate", "lbmc_init", "lbmc_iterate",
                      "lbmc_fetch", "lbmc_destroy", "lbmc_get_step", "lbmc_set_stream",
                      "lbmc_synchronize", "lbmc_classify", "lbmc_lattice_tables"):
@@ -149,7 +152,7 @@ class _Keep:
 def make_config(lattice, length, tau=1.0, tau_mrt=(), c_smag=0.0, collision_type=BGK,
                 forcing=False, macro_bc=False, micro_bc=False, init_type=INIT_STATIC,
                 storage=F32, compat=0, storage_scale=0.0, device=0, streaming=STREAM_SHIFT,
-                tolerance=0.0) -> Config:
+                tolerance=0.0, kernel=KERNEL_AUTO) -> Config:
     lat = LATTICE_IDS.get(lattice, lattice)
     cfg = Config()
     check(library().lbmc_config_default(ctypes.byref(cfg), lat))
@@ -172,6 +175,7 @@ def make_config(lattice, length, tau=1.0, tau_mrt=(), c_smag=0.0, collision_type
     cfg.device = device
     cfg.streaming = streaming
     cfg.tolerance = tolerance
+    cfg.kernel = kernel
     return cfg
 
 

@@ -30,6 +30,14 @@ def err(a, b):
     return float(np.abs(a - b).max() / (scale if scale > 0 else 1.0))
 
 
+KERNELS = ["direct", "pipelined"]
+
+
+def kernel_id(lbmc, name):
+    return {"direct": lbmc.KERNEL_DIRECT, "pipelined": lbmc.KERNEL_PIPELINED,
+            "auto": lbmc.KERNEL_AUTO}[name]
+
+
 def run_engine(lbmc, case, steps, storage="f32", **kw):
     with lbmc.Engine.from_case(case, storage=lbmc.STORAGE_IDS[storage], **kw) as eng:
         eng.iterate(steps, lbmc.STORE_MACROS | lbmc.SYNC)
@@ -52,12 +60,18 @@ COMBOS = [(lat, ct, forcing, bc, smag)
           for bc in (None, "random", "zh") for smag in (0.0, 0.1) if not (smag and ct >= 2)]
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("compat", ["patched", "asis"])
 @pytest.mark.parametrize("lat,ct,forcing,bc,smag", COMBOS)
-def test_engine_matches_restatement(lbmc, lat, ct, forcing, bc, smag, compat):
+def test_engine_matches_restatement(lbmc, lat, ct, forcing, bc, smag, compat, kernel):
     if smag and compat == "asis":
         pytest.skip("the reference's Smagorinsky is undefined as is (q_bar uninitialised)")
-    length = (37, 21, 1) if lat == "d2q9" else (19, 11, 9)
+    # Rows of 40 (D2Q9) / 24 (D3Q15) elements are whole 16-byte granules in
+    # every storage, so the bulk-copy pipeline takes them; 37 / 19 are not.
+    if kernel == "pipelined":
+        length = (40, 21, 1) if lat == "d2q9" else (24, 11, 9)
+    else:
+        length = (37, 21, 1) if lat == "d2q9" else (19, 11, 9)
     case = make_case(lat, length, ct, forcing, solids=0.08, partial=0.15 if ct % 2 else 0.0,
                      macro="random" if bc == "random" else None,
                      micro="zh" if bc == "zh" else None, c_smag=smag, seed=7 + ct,
@@ -71,23 +85,27 @@ def test_engine_matches_restatement(lbmc, lat, ct, forcing, bc, smag, compat):
     r.run(steps)
     rr, ur = r.macros()
     for storage in ("f64", "f32"):
-        fg, rg, ug = run_engine(lbmc, case, steps, storage)
+        fg, rg, ug = run_engine(lbmc, case, steps, storage, kernel=kernel_id(lbmc, kernel))
         tol = TOL[storage]
         assert err(fg, r.f()) <= tol, storage
         assert err(rg, rr) <= tol, storage
         assert err(ug, ur) <= tol, storage
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("lat", ["d2q9", "d3q15"])
-def test_stress_free_faces(lbmc, lat):
+def test_stress_free_faces(lbmc, lat, kernel):
     """Stress-free micro BCs (codes 5-8 / 7-12) with the intended semantics:
     copy the inward post-streaming populations of the interior neighbour."""
-    length = (23, 14, 1) if lat == "d2q9" else (13, 9, 8)
+    if kernel == "pipelined":
+        length = (24, 14, 1) if lat == "d2q9" else (16, 9, 8)
+    else:
+        length = (23, 14, 1) if lat == "d2q9" else (13, 9, 8)
     case = make_case(lat, length, 0, True, solids=0.05, micro="sf", seed=3)
     r = Restatement(case)
     r.run(40)
     rr, ur = r.macros()
-    fg, rg, ug = run_engine(lbmc, case, 40, "f64")
+    fg, rg, ug = run_engine(lbmc, case, 40, "f64", kernel=kernel_id(lbmc, kernel))
     assert err(fg, r.f()) <= TOL["f64"]
     assert err(ug, ur) <= TOL["f64"]
 
@@ -95,7 +113,7 @@ def test_stress_free_faces(lbmc, lat):
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
 @pytest.mark.parametrize("lat,ct", [("d2q9", 0), ("d2q9", 3), ("d3q15", 2), ("d3q15", 1)])
 def test_reduced_precision_storage(lbmc, lat, ct, storage):
-    """f - w stored as FP16/BF16 with FP32 arithmetic, against FP64."""
+    """FP16/BF16 storage; the sizes take the bulk-copy pipeline."""
     length = (40, 24, 1) if lat == "d2q9" else (16, 12, 10)
     case = make_case(lat, length, ct, True, solids=0.05, partial=0.1 if ct % 2 else 0.0,
                      seed=5)
@@ -107,8 +125,9 @@ def test_reduced_precision_storage(lbmc, lat, ct, storage):
     assert err(rg - 1, rr - 1) <= TOL[storage]
 
 
-def test_step_counter_continues_across_calls(lbmc):
-    case = make_case("d3q15", (11, 7, 6), 2, True, solids=0.1, micro="zh", seed=9)
+@pytest.mark.parametrize("length", [(11, 7, 6), (16, 7, 6)])
+def test_step_counter_continues_across_calls(lbmc, length):
+    case = make_case("d3q15", length, 2, True, solids=0.1, micro="zh", seed=9)
     with lbmc.Engine.from_case(case) as a, lbmc.Engine.from_case(case) as b:
         a.iterate(13, lbmc.SYNC)
         for k in (4, 1, 8):
@@ -204,3 +223,31 @@ def test_init_equilibrium(lbmc):
     expect = Restatement(case).equilibrium(rho, u)
     with lbmc.Engine.from_case(case, init_type=lbmc.INIT_EQUILIBRIUM, storage=lbmc.F64) as eng:
         np.testing.assert_allclose(eng.f(), expect, rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+def test_pipelined_and_direct_kernels_agree(lbmc, storage):
+    """The two step kernels compute the same thing: identical bits."""
+    case = make_case("d3q15", (32, 20, 12), 3, True, solids=0.1, partial=0.1, micro="zh",
+                     macro="random", seed=12)
+    a = run_engine(lbmc, case, 25, storage, kernel=lbmc.KERNEL_DIRECT)
+    b = run_engine(lbmc, case, 25, storage, kernel=lbmc.KERNEL_PIPELINED)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_pipelined_rejects_ragged_rows(lbmc):
+    case = make_case("d3q15", (19, 8, 8), seed=1)
+    with pytest.raises(lbmc.LbmcError) as ei:
+        lbmc.Engine.from_case(case, kernel=lbmc.KERNEL_PIPELINED)
+    assert ei.value.status == lbmc.ERR_UNSUPPORTED
+
+
+def test_device_wait_timeout_is_reported(lbmc):
+    """Failure detection without a GPU fault: a barrier nobody signals; the
+    bounded wait gives up after 50 ms and the status comes back, after which
+    the device still runs a normal step."""
+    assert lbmc.library().lbmc_selftest_wait_timeout(0, 0.05) == lbmc.ERR_TIMEOUT
+    case = make_case("d2q9", (16, 8, 1), seed=2)
+    _, rho, _ = run_engine(lbmc, case, 3)
+    assert np.isfinite(rho).all()
