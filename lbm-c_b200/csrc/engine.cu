@@ -445,6 +445,8 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     TRYCUDA(cudaMemset(d.sf_buf, 0, (size_t)cs * q * d.n_sf), "clear sf");
   }
 
+  TRY(dev_alloc(h, &d.table_dev, sizeof(d.table), "class table"));
+  TRYCUDA(cudaMemcpy(d.table_dev, d.table, sizeof(d.table), cudaMemcpyHostToDevice), "upload class table");
   TRY(dev_alloc(h, &d.error_flag, sizeof(unsigned), "error flag"));
   TRYCUDA(cudaMemset(d.error_flag, 0, sizeof(unsigned)), "clear error flag");
   {

@@ -33,6 +33,7 @@ struct DeviceState {
   int forcing;
   int blend;  // Noble-Torczynski partial nodes present
   uint16_t table[256];
+  uint16_t *table_dev;      // device copy of table
   unsigned *error_flag;     // device word, ERROR_TIMEOUT on an expired wait
   long long timeout_cycles; // bound of every device-side wait
   int pipeline;             // allow the bulk-copy pipelined kernel

@@ -41,7 +41,7 @@ struct Launchers {
     a.timeout_cycles = d.timeout_cycles;
     a.rows = (long long)d.L[1] * d.L[2];
     a.stages = d.stages;
-    for (int k = 0; k < 256; k++) a.table[k] = d.table[k];
+    a.table = d.table_dev;
     return a;
   }
 
@@ -65,14 +65,15 @@ struct Launchers {
     return d.pipeline && (d.L[0] * sizeof(S)) % 16 == 0 && 2 * stage_bytes(d) <= 200 * 1024;
   }
   static int pipe_stages(const DeviceState &d) {
-    long long st = (64 * 1024) / (long long)stage_bytes(d);
+    long long st = (96 * 1024) / (long long)stage_bytes(d);
     if (st < 2) st = 2;
     if (st > PIPE_MAX_STAGES) st = PIPE_MAX_STAGES;
     return (int)st;
   }
+  // One producer warp plus up to STEP_BLOCK / 32 consumer warps.
   static int pipe_threads(const DeviceState &d) {
     int bx = (d.L[0] + 31) / 32 * 32;
-    return bx < STEP_BLOCK ? bx : STEP_BLOCK;
+    return 32 + (bx < STEP_BLOCK ? bx : STEP_BLOCK);
   }
 
   template <int COL, bool FORCE, bool BLEND, bool DIAG>

@@ -48,27 +48,46 @@ struct Storage;
 template <>
 struct Storage<double> {
   using C = double;
+  static constexpr bool SCALED = false;
   static __device__ __forceinline__ C get(const double *p) { return *p; }
   static __device__ __forceinline__ void put(double *p, C v) { *p = v; }
 };
 template <>
 struct Storage<float> {
   using C = float;
+  static constexpr bool SCALED = false;
   static __device__ __forceinline__ C get(const float *p) { return *p; }
   static __device__ __forceinline__ void put(float *p, C v) { *p = v; }
 };
+// FP16 keeps (f - w) * scale so that small deviations stay out of the
+// subnormal range; BF16 has FP32's exponent range and needs no scale.
 template <>
 struct Storage<__half> {
   using C = float;
+  static constexpr bool SCALED = true;
   static __device__ __forceinline__ C get(const __half *p) { return __half2float(*p); }
   static __device__ __forceinline__ void put(__half *p, C v) { *p = __float2half_rn(v); }
 };
 template <>
 struct Storage<__nv_bfloat16> {
   using C = float;
+  static constexpr bool SCALED = false;
   static __device__ __forceinline__ C get(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
   static __device__ __forceinline__ void put(__nv_bfloat16 *p, C v) { *p = __float2bfloat16_rn(v); }
 };
+
+// Stored-value conversions with the storage scale applied only where the
+// format uses one.
+template <class S>
+__device__ __forceinline__ typename Storage<S>::C load_dev(const S *p, typename Storage<S>::C inv_scale) {
+  if constexpr (Storage<S>::SCALED) return Storage<S>::get(p) * inv_scale;
+  else return Storage<S>::get(p);
+}
+template <class S>
+__device__ __forceinline__ void store_dev(S *p, typename Storage<S>::C v, typename Storage<S>::C scale) {
+  if constexpr (Storage<S>::SCALED) Storage<S>::put(p, v * scale);
+  else Storage<S>::put(p, v);
+}
 
 // ------------------------------------------------------------ node classes
 
@@ -123,7 +142,7 @@ struct StepArgs {
   long long timeout_cycles;     // limit of every device-side wait
   long long rows;               // Ly * Lz (pipelined kernel)
   int stages;                   // shared-memory stages (pipelined kernel)
-  uint16_t table[256];
+  const uint16_t *table;        // 256 class-table entries (device memory)
 };
 
 constexpr unsigned ERROR_TIMEOUT = 1u;
@@ -659,7 +678,7 @@ __device__ __forceinline__ void store_and_reduce(const Node<L, C> &nd, const Ste
 template <class C>
 __device__ __forceinline__ void block_diag(const double (&v)[DIAG_VALUES], bool nonfinite,
                                            const StepArgs<C> &a, long long block) {
-  __shared__ double red[STEP_BLOCK / 32][DIAG_VALUES];
+  __shared__ double red[16][DIAG_VALUES];  // up to 512 threads
   double s[DIAG_VALUES];
 #pragma unroll
   for (int k = 0; k < DIAG_VALUES; k++) {
@@ -690,7 +709,7 @@ __device__ __forceinline__ void block_diag(const double (&v)[DIAG_VALUES], bool 
 // Grid: blockDim (bx, 1, 1) along x, gridDim (ceil(Lx/bx), Ly, Lz).
 template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG>
 __global__ void __launch_bounds__(STEP_BLOCK)
-    step_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a) {
+    step_kernel(const StepArgs<typename Storage<S>::C> a) {
   using C = typename Storage<S>::C;
   constexpr int Q = L::Q;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -699,6 +718,7 @@ __global__ void __launch_bounds__(STEP_BLOCK)
   double dv[DIAG_VALUES] = {0, 0, 0, 0, 0};
   bool nonfinite = false;
   if (active) {
+    const C inv_scale = a.inv_scale, scale = a.scale;
     Sites st;
     st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
     const int n = x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z);
@@ -706,7 +726,7 @@ __global__ void __launch_bounds__(STEP_BLOCK)
     Node<L, C> nd;
     unroll<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      nd.g[i] = Storage<S>::get(f + i * a.pitch + st.template slot<L>(i)) * a.inv_scale;
+      nd.g[i] = load_dev(f + i * a.pitch + st.template slot<L>(i), inv_scale);
     });
     const int cls = a.cls[n];
     C out[Q];
@@ -718,7 +738,7 @@ __global__ void __launch_bounds__(STEP_BLOCK)
     }
     unroll<Q>([&](auto ic) {
       constexpr int i = decltype(ic)::value;
-      Storage<S>::put(f + i * a.pitch + st.template slot<L>(i), out[i] * a.scale);
+      store_dev(f + i * a.pitch + st.template slot<L>(i), out[i], scale);
     });
     store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
   }
@@ -831,104 +851,149 @@ __device__ __forceinline__ void issue_row_store(S *f, long long pitch, long long
 
 constexpr int PIPE_MAX_STAGES = 8;
 
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Warp-specialised pipeline.  Warp 0 is the producer: its lane 0 issues the
+// bulk loads of row k into stage k % stages (completion counted on
+// full[stage]), and once the consumer warps have signalled done[stage] it
+// bulk-stores the row back and reuses the stage for row k + stages.  Warps
+// 1.. are consumers: they wait on full[stage], collide the row's nodes in
+// shared memory, fence their writes for the async proxy and arrive on
+// done[stage].  Every wait is bounded (timeout_cycles); on expiry the kernel
+// records ERROR_TIMEOUT, stops issuing work, drains its own copies with
+// bounded waits and returns.
 // Dynamic shared memory: [stages][Q][Lx] storage elements.
 template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG>
-__global__ void __launch_bounds__(STEP_BLOCK)
-    step_pipelined_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a) {
+__global__ void __launch_bounds__(STEP_BLOCK + 32)
+    step_pipelined_kernel(const StepArgs<typename Storage<S>::C> a) {
   using C = typename Storage<S>::C;
   constexpr int Q = L::Q;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long full_bar[PIPE_MAX_STAGES];
-  __shared__ int abort_flag;
+  __shared__ __align__(8) unsigned long long done_bar[PIPE_MAX_STAGES];
+  __shared__ volatile int abort_flag;
   S *buf = reinterpret_cast<S *>(smem_raw);
   const int lx = a.L[0];
   const int nst = a.stages;
-  const long long stage_elems = (long long)Q * lx;
-  S *f = reinterpret_cast<S *>(a.f);
+  const int stage_elems = Q * lx;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int consumers = (int)(blockDim.x >> 5) - 1;
   const long long rows = a.rows;
   const long long my_rows = rows > blockIdx.x ? (rows - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  const bool leader = threadIdx.x == 0;
+  const long long tmo = a.timeout_cycles;
 
-  if (leader) {
-    for (int k = 0; k < nst; k++) mbar_init(smem_addr(&full_bar[k]), 1);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < nst; k++) {
+      mbar_init(smem_addr(&full_bar[k]), 1);
+      mbar_init(smem_addr(&done_bar[k]), consumers);
+    }
     mbar_fence_init();
     abort_flag = 0;
   }
   __syncthreads();
-  if (leader) {
-    for (long long k = 0; k < nst - 1 && k < my_rows; k++)
-      issue_row_load<L>(f, a.pitch, blockIdx.x + k * gridDim.x, a.s, a.L, buf + (k % nst) * stage_elems,
-                        smem_addr(&full_bar[k % nst]));
-  }
-  // x positions of this thread's nodes along the row, and their shifted slots
+
   double dv[DIAG_VALUES] = {0, 0, 0, 0, 0};
   bool nonfinite = false;
-  long long k = 0;
-  for (; k < my_rows; k++) {
-    const int st_idx = (int)(k % nst);
-    const unsigned parity = (unsigned)((k / nst) & 1);
-    if (!mbar_wait_bounded(smem_addr(&full_bar[st_idx]), parity, a.timeout_cycles)) {
-      atomicOr(a.error_flag, ERROR_TIMEOUT);
-      abort_flag = 1;
-    }
-    __syncthreads();
-    if (abort_flag) break;
-    const long long row = blockIdx.x + k * gridDim.x;
-    const int y = (int)(row % a.L[1]), z = (int)(row / a.L[1]);
-    S *sb = buf + st_idx * stage_elems;
-    for (int x = threadIdx.x; x < lx; x += blockDim.x) {
-      const int xp = wrap_sub(x, a.s[0], lx);  // e_x = +1 reads x - s
-      const int xm = wrap_add(x, a.s[0], lx);  // e_x = -1 reads x + s
-      const int n = x + lx * (y + a.L[1] * z);
-      Node<L, C> nd;
-      unroll<Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        constexpr int ex = L::e(0, i);
-        const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
-        nd.g[i] = Storage<S>::get(sb + i * lx + xs) * a.inv_scale;
-      });
-      const int cls = a.cls[n];
-      C out[Q];
-      if (cls == CLASS_SOLID) {
-        collide_solid(nd, out);
-      } else {
-        moments(nd);
-        collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
+
+  if (warp == 0) {
+    if (lane == 0) {
+      S *f = reinterpret_cast<S *>(a.f);
+      long long issued = 0;  // rows whose loads were issued
+      long long k = 0;
+      for (; k < my_rows; k++) {
+        const int st_idx = (int)(k % nst);
+        if (k >= nst) {
+          // Stage st_idx holds row k - nst: store it once the consumers are done.
+          const long long prev = k - nst;
+          if (!mbar_wait_bounded(smem_addr(&done_bar[st_idx]), (unsigned)((prev / nst) & 1), tmo)) {
+            atomicOr(a.error_flag, ERROR_TIMEOUT);
+            abort_flag = 1;
+            break;
+          }
+          issue_row_store<L>(f, a.pitch, blockIdx.x + prev * gridDim.x, a.s, a.L, buf + st_idx * stage_elems);
+          bulk_wait_read<0>();
+        }
+        if (abort_flag) break;
+        issue_row_load<L>(f, a.pitch, blockIdx.x + k * gridDim.x, a.s, a.L, buf + st_idx * stage_elems,
+                          smem_addr(&full_bar[st_idx]));
+        issued = k + 1;
       }
-      unroll<Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        constexpr int ex = L::e(0, i);
-        const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
-        Storage<S>::put(sb + i * lx + xs, out[i] * a.scale);
-      });
-      store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
-    }
-    fence_proxy_async();
-    __syncthreads();
-    if (leader) {
-      issue_row_store<L>(f, a.pitch, row, a.s, a.L, sb);
-      // The stage that held row k-1 is refilled with row k + nst - 1 once its
-      // store has finished reading shared memory.
-      const long long next = k + nst - 1;
-      if (next < my_rows) {
-        bulk_wait_read<1>();
-        const int ns = (int)(next % nst);
-        issue_row_load<L>(f, a.pitch, blockIdx.x + next * gridDim.x, a.s, a.L, buf + ns * stage_elems,
-                          smem_addr(&full_bar[ns]));
+      // Store the rows still resident (the last `nst` of this block).
+      if (!abort_flag) {
+        const long long first = my_rows > nst ? my_rows - nst : 0;
+        for (long long j = first; j < my_rows; j++) {
+          const int st_idx = (int)(j % nst);
+          if (!mbar_wait_bounded(smem_addr(&done_bar[st_idx]), (unsigned)((j / nst) & 1), tmo)) {
+            atomicOr(a.error_flag, ERROR_TIMEOUT);
+            abort_flag = 1;
+            break;
+          }
+          issue_row_store<L>(f, a.pitch, blockIdx.x + j * gridDim.x, a.s, a.L, buf + st_idx * stage_elems);
+        }
       }
+      bulk_wait_all();
+      if (abort_flag) {
+        // Loads issued but possibly never consumed: wait (bounded) for them so
+        // no copy still targets this block's shared memory at exit.
+        const long long first = issued > nst ? issued - nst : 0;
+        for (long long j = first; j < issued; j++)
+          mbar_wait_bounded(smem_addr(&full_bar[j % nst]), (unsigned)((j / nst) & 1), tmo);
+      }
+    }
+  } else {
+    const C inv_scale = a.inv_scale, scale = a.scale;
+    const int ctid = threadIdx.x - 32;
+    const int cstride = consumers * 32;
+    for (long long k = 0; k < my_rows; k++) {
+      const int st_idx = (int)(k % nst);
+      if (abort_flag) break;
+      if (!mbar_wait_bounded(smem_addr(&full_bar[st_idx]), (unsigned)((k / nst) & 1), tmo)) {
+        atomicOr(a.error_flag, ERROR_TIMEOUT);
+        abort_flag = 1;
+        break;
+      }
+      const long long row = blockIdx.x + k * gridDim.x;
+      const int y = (int)(row % a.L[1]), z = (int)(row / a.L[1]);
+      S *sb = buf + st_idx * stage_elems;
+      const int nrow = lx * (y + a.L[1] * z);
+      for (int x = ctid; x < lx; x += cstride) {
+        const int xp = wrap_sub(x, a.s[0], lx);  // e_x = +1 reads x - s
+        const int xm = wrap_add(x, a.s[0], lx);  // e_x = -1 reads x + s
+        const int n = x + nrow;
+        Node<L, C> nd;
+        unroll<Q>([&](auto ic) {
+          constexpr int i = decltype(ic)::value;
+          constexpr int ex = L::e(0, i);
+          const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
+          nd.g[i] = load_dev(sb + i * lx + xs, inv_scale);
+        });
+        const int cls = a.cls[n];
+        C out[Q];
+        if (cls == CLASS_SOLID) {
+          collide_solid(nd, out);
+        } else {
+          moments(nd);
+          collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
+        }
+        unroll<Q>([&](auto ic) {
+          constexpr int i = decltype(ic)::value;
+          constexpr int ex = L::e(0, i);
+          const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
+          store_dev(sb + i * lx + xs, out[i], scale);
+        });
+        store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
+      }
+      fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_addr(&done_bar[st_idx]));
     }
   }
-  if (leader) {
-    bulk_wait_all();
-    if (abort_flag) {
-      // Drain loads that were issued but not consumed (bounded), so no copy
-      // still targets this block's shared memory when it exits.
-      for (long long j = k; j < my_rows && j < k + nst; j++) {
-        mbar_wait_bounded(smem_addr(&full_bar[j % nst]), (unsigned)((j / nst) & 1), a.timeout_cycles);
-      }
-    }
+  if (DIAG) {
+    __syncthreads();
+    block_diag<C>(dv, nonfinite, a, blockIdx.x);
   }
-  if (DIAG) block_diag<C>(dv, nonfinite, a, blockIdx.x);
 }
 
 // Stress-free pre-pass: before the step, copy the inward populations of each
@@ -936,7 +1001,7 @@ __global__ void __launch_bounds__(STEP_BLOCK)
 // neighbour's shift slots) into sf_buf, so the step kernel can use them
 // without racing with the neighbour's in-place update.
 template <class L, class S>
-__global__ void sf_gather_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a,
+__global__ void sf_gather_kernel(const StepArgs<typename Storage<S>::C> a,
                                  const int *sf_nodes, const uint8_t *sf_face_of, int n_sf,
                                  typename Storage<S>::C *sf_buf) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -963,14 +1028,14 @@ __global__ void sf_gather_kernel(const __grid_constant__ StepArgs<typename Stora
     });
     if (need)
       sf_buf[(long long)k * L::Q + i] =
-          Storage<S>::get(f + i * a.pitch + st.template slot<L>(i)) * a.inv_scale;
+          load_dev(f + i * a.pitch + st.template slot<L>(i), a.inv_scale);
   });
 }
 
 // Natural-layout FP64 copy of population i: out[x] = w_i + g_i(x).
 // Grid as for the direct step kernel.
 template <class L, class S>
-__global__ void fetch_population_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a,
+__global__ void fetch_population_kernel(const StepArgs<typename Storage<S>::C> a,
                                         int i, double *out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= a.L[0]) return;
@@ -981,14 +1046,14 @@ __global__ void fetch_population_kernel(const __grid_constant__ StepArgs<typenam
   unroll<L::Q>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     if (k == i)
-      out[n] = weight<L>(k) + (double)(Storage<S>::get(f + k * a.pitch + st.template slot<L>(k)) * a.inv_scale);
+      out[n] = weight<L>(k) + (double)load_dev(f + k * a.pitch + st.template slot<L>(k), a.inv_scale);
   });
 }
 
 // Writes population i from natural-layout FP64 values into its slots for
 // the current step: stored = (f - w) * scale.
 template <class L, class S>
-__global__ void upload_population_kernel(const __grid_constant__ StepArgs<typename Storage<S>::C> a,
+__global__ void upload_population_kernel(const StepArgs<typename Storage<S>::C> a,
                                          int i, const double *in) {
   using C = typename Storage<S>::C;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1000,7 +1065,7 @@ __global__ void upload_population_kernel(const __grid_constant__ StepArgs<typena
   unroll<L::Q>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
     if (k == i)
-      Storage<S>::put(f + k * a.pitch + st.template slot<L>(k), (C)(in[n] - weight<L>(k)) * a.scale);
+      store_dev(f + k * a.pitch + st.template slot<L>(k), (C)(in[n] - weight<L>(k)), a.scale);
   });
 }
 

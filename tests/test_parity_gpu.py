@@ -77,9 +77,10 @@ def test_engine_matches_restatement(lbmc, lat, ct, forcing, bc, smag, compat, ke
                      micro="zh" if bc == "zh" else None, c_smag=smag, seed=7 + ct,
                      compat=COMPAT_AS_IS if compat == "asis" else 0)
     steps = 60
-    if compat == "asis" and lat == "d3q15" and ct >= 2:
-        # As is, D3Q15 MRT relaxes nothing (M_inv = 0): with no dissipation the
-        # FP32 rounding differences grow, so this case is compared early.
+    if compat == "asis" and lat == "d3q15" and (ct >= 2 or bc == "zh"):
+        # As is, D3Q15 MRT relaxes nothing (M_inv = 0) and the +z Zou-He face
+        # uses u_x = 0: with no dissipation, or a face that injects mass, the
+        # FP32 rounding differences grow, so these cases are compared early.
         steps = 10
     r = Restatement(case)
     r.run(steps)
