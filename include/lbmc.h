@@ -126,9 +126,11 @@ typedef struct lbmc_config {
   int reserved[5];
 } lbmc_config;
 
-/* Step-kernel choice (lbmc_config.kernel).  AUTO takes the bulk-copy
- * pipeline whenever a row of one population is a whole number of 16-byte
- * granules and fits the shared-memory stages, else the direct-load kernel. */
+/* Step-kernel choice (lbmc_config.kernel).  AUTO and DIRECT run the
+ * direct-load kernel; PIPELINED runs the bulk-copy (TMA) row pipeline, which
+ * needs a population row to be a whole number of 16-byte granules and two
+ * shared-memory stages of Q rows to fit (else lbmc_init fails with
+ * LBMC_ERR_UNSUPPORTED). */
 typedef enum lbmc_kernel {
   LBMC_KERNEL_AUTO = 0,
   LBMC_KERNEL_DIRECT = 1,

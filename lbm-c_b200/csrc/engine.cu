@@ -379,6 +379,12 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   d.scale = cfg->storage_scale > 0 ? cfg->storage_scale : default_scale(cfg->storage);
   d.compat = cfg->compat;
   d.col = cfg->collision_type >= LBMC_MRT ? COL_MRT : (cfg->c_smag > 0 ? COL_BGK_SMAG : COL_BGK);
+  if (d.col == COL_MRT) {
+    bool conserved_zero = true;
+    for (int k = 0; k < q; k++)
+      if ((k == 0 || k == 3 || k == 5 || (q == 15 && k == 7)) && cfg->tau_mrt[k] != 0.0) conserved_zero = false;
+    if (conserved_zero) d.col = COL_MRT_NC;
+  }
   d.forcing = cfg->forcing ? 1 : 0;
   d.blend = hc.any_partial ? 1 : 0;
 
@@ -455,7 +461,7 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     // Every device-side wait gives up after about two seconds.
     d.timeout_cycles = (long long)(khz > 0 ? khz : 2000000) * 1000LL * 2;
   }
-  d.pipeline = cfg->kernel != LBMC_KERNEL_DIRECT;
+  d.pipeline = cfg->kernel == LBMC_KERNEL_PIPELINED ? 2 : 0;
   TRYCUDA(h->ops->plan(d), "kernel planning");
   if (cfg->kernel == LBMC_KERNEL_PIPELINED && !d.use_pipeline) {
     release(h);

@@ -31,7 +31,8 @@ struct Launchers {
     a.diag_flag = d.flag;
     a.n = (int)d.n;
     a.tau = (C)d.tau;
-    for (int k = 0; k < 15; k++) a.s_mrt[k] = (C)d.s_mrt[k];
+    // MRT rates pre-divided by the moment norms D_k = sum_i M_ki^2.
+    for (int k = 0; k < 15; k++) a.s_mrt[k] = k < L::Q ? (C)(d.s_mrt[k] / (double)L::mnorm(k)) : C(0);
     a.c_smag = (C)d.c_smag;
     a.scale = (C)d.scale;
     a.inv_scale = (C)(1.0 / d.scale);
@@ -122,6 +123,7 @@ struct Launchers {
     switch (d.col) {
       case COL_BGK: e = launch_col<COL_BGK>(a, d, diag, st); break;
       case COL_BGK_SMAG: e = launch_col<COL_BGK_SMAG>(a, d, diag, st); break;
+      case COL_MRT_NC: e = launch_col<COL_MRT_NC>(a, d, diag, st); break;
       default: e = launch_col<COL_MRT>(a, d, diag, st); break;
     }
     if (e != cudaSuccess) return e;
@@ -131,7 +133,9 @@ struct Launchers {
   // Chooses the kernel and its launch geometry for a handle (called once by
   // lbmc_init after the device state is filled in).
   static cudaError_t plan(DeviceState &d) {
-    d.use_pipeline = pipelined_eligible(d) ? 1 : 0;
+    // The direct-load kernel is the default; the bulk-copy pipeline runs when
+    // asked for (lbmc_config.kernel) and the rows allow it.
+    d.use_pipeline = (d.pipeline == 2 && pipelined_eligible(d)) ? 1 : 0;
     if (!d.use_pipeline) {
       d.nblocks = blocks(d);
       return cudaSuccess;
@@ -149,6 +153,7 @@ struct Launchers {
     switch (d.col) {
       case COL_BGK: probe(step_pipelined_kernel<L, S, COL_BGK, true, true, true>); break;
       case COL_BGK_SMAG: probe(step_pipelined_kernel<L, S, COL_BGK_SMAG, true, true, true>); break;
+      case COL_MRT_NC: probe(step_pipelined_kernel<L, S, COL_MRT_NC, true, true, true>); break;
       default: probe(step_pipelined_kernel<L, S, COL_MRT, true, true, true>); break;
     }
     if (e != cudaSuccess) return e;

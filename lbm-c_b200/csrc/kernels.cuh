@@ -111,6 +111,13 @@ constexpr unsigned COMPAT_MRTPOR_INPLACE = 1u << 3;
 constexpr int COL_BGK = 0;
 constexpr int COL_BGK_SMAG = 1;
 constexpr int COL_MRT = 2;
+constexpr int COL_MRT_NC = 3;  // MRT whose rates on rho and j are zero
+
+// rho and the momentum components (the conserved moments).
+template <class L>
+__host__ __device__ constexpr bool moment_conserved(int k) {
+  return k == 0 || k == 3 || k == 5 || (L::Q == 15 && k == 7);
+}
 
 constexpr int DIAG_VALUES = 5;  // mass, momentum x/y/z, kinetic energy
 constexpr int STEP_BLOCK = 256;
@@ -165,22 +172,27 @@ __host__ __device__ constexpr int sel(int e) { return e == 0 ? 0 : (e > 0 ? 1 : 
 // (LBM-C/solver.cu:82-94).  Index [1] of a component is e = +1 (reads
 // x - s), [2] is e = -1 (reads x + s).  The kernels launch one block row per
 // (y, z), so the row offsets are uniform across the block.
+// Slots are unsigned 32-bit element offsets within one population array, so
+// each access is one 32x32+64 multiply-add on the population's base pointer.
 struct Sites {
-  int x[3];
-  int row[3][3];  // [sel(e_y)][sel(e_z)] -> Lx * (y' + Ly * z')
+  unsigned x[3];
+  unsigned row[3][3];  // [sel(e_y)][sel(e_z)] -> Lx * (y' + Ly * z')
   __device__ __forceinline__ void init(int cx, int cy, int cz, const int *s, const int *L) {
     x[0] = cx;
     x[1] = wrap_sub(cx, s[0], L[0]);
     x[2] = wrap_add(cx, s[0], L[0]);
-    const int ys[3] = {cy, wrap_sub(cy, s[1], L[1]), wrap_add(cy, s[1], L[1])};
-    const int zs[3] = {cz, wrap_sub(cz, s[2], L[2]), wrap_add(cz, s[2], L[2])};
+    const unsigned ys[3] = {(unsigned)cy, (unsigned)wrap_sub(cy, s[1], L[1]),
+                            (unsigned)wrap_add(cy, s[1], L[1])};
+    const unsigned zs[3] = {(unsigned)cz, (unsigned)wrap_sub(cz, s[2], L[2]),
+                            (unsigned)wrap_add(cz, s[2], L[2])};
+    const unsigned lx = L[0], ly = L[1];
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
-      for (int b = 0; b < 3; b++) row[a][b] = L[0] * (ys[a] + L[1] * zs[b]);
+      for (int b = 0; b < 3; b++) row[a][b] = lx * (ys[a] + ly * zs[b]);
   }
   template <class L>
-  __device__ __forceinline__ int slot(int i) const {
+  __device__ __forceinline__ unsigned slot(int i) const {
     // i is a compile-time constant after unrolling, so sel() folds.
     return x[sel(L::e(0, i))] + row[sel(L::e(1, i))][sel(L::e(2, i))];
   }
@@ -448,6 +460,102 @@ __device__ __forceinline__ C meq_dev(int k, const Node<L, C> &nd, unsigned compa
   }
 }
 
+// D3Q15 MRT relaxation with the moment transforms written as butterflies.
+// With S_p = g_i + g_opp(i), D_p = g_i - g_opp(i) for the pairs
+// p = 1 (x), 3 (y), 5 (z), 7 (+++), 8 (-++), 9 (+-+), 10 (--+), the rows of
+// M (LBM-C/macros.cu:77-95) on the four diagonal pairs are a 4x4 Hadamard
+// pattern, so M g and M^T m* each take a few dozen additions instead of the
+// ~200 of the dense product.  ms[k] = (s_k / D_k)(m_k - meq_k); NC skips the
+// conserved moments (0, 3, 5, 7) whose rates are zero.  acc = M^T ms.
+template <class C, bool NC>
+__device__ __forceinline__ void mrt_d3q15(const Node<D3Q15, C> &nd, const C *srate, unsigned compat,
+                                          C (&acc)[15]) {
+  const C *g = nd.g;
+  const C S1 = g[1] + g[2], D1 = g[1] - g[2];
+  const C S3 = g[3] + g[4], D3 = g[3] - g[4];
+  const C S5 = g[5] + g[6], D5 = g[5] - g[6];
+  const C S7 = g[7] + g[14], D7 = g[7] - g[14];
+  const C S8 = g[8] + g[13], D8 = g[8] - g[13];
+  const C S9 = g[9] + g[12], D9 = g[9] - g[12];
+  const C S10 = g[10] + g[11], D10 = g[10] - g[11];
+  // forward
+  const C Sa = S1 + S3 + S5;
+  const C bA = S7 + S8, bB = S7 - S8, bC = S9 + S10, bD = S9 - S10;
+  const C Sd = bA + bC, m12 = bA - bC, m13 = bB + bD, m11 = bB - bD;
+  const C da = D7 + D8, db = D7 - D8, dc = D9 + D10, dd = D9 - D10;
+  const C Zd = da + dc, Yd = da - dc, Xd = db + dd, m14 = db - dd;
+  const C m1 = Sd - Sa - C(2) * g[0];
+  const C m2 = Sd - C(4) * Sa + C(16) * g[0];
+  const C m4 = Xd - C(4) * D1;
+  const C m6 = Yd - C(4) * D3;
+  const C m8 = Zd - C(4) * D5;
+  const C m9 = C(2) * S1 - S3 - S5;
+  const C m10 = S3 - S5;
+  // relaxed, scaled moment deviations
+  const C ms1 = srate[1] * (m1 - meq_dev<D3Q15>(1, nd, compat));
+  const C ms2 = srate[2] * (m2 - meq_dev<D3Q15>(2, nd, compat));
+  const C ms4 = srate[4] * (m4 - meq_dev<D3Q15>(4, nd, compat));
+  const C ms6 = srate[6] * (m6 - meq_dev<D3Q15>(6, nd, compat));
+  const C ms8 = srate[8] * (m8 - meq_dev<D3Q15>(8, nd, compat));
+  const C ms9 = srate[9] * (m9 - meq_dev<D3Q15>(9, nd, compat));
+  const C ms10 = srate[10] * (m10 - meq_dev<D3Q15>(10, nd, compat));
+  const C ms11 = srate[11] * (m11 - meq_dev<D3Q15>(11, nd, compat));
+  const C ms12 = srate[12] * (m12 - meq_dev<D3Q15>(12, nd, compat));
+  const C ms13 = srate[13] * (m13 - meq_dev<D3Q15>(13, nd, compat));
+  const C ms14 = srate[14] * (m14 - meq_dev<D3Q15>(14, nd, compat));
+  // inverse: acc = M^T ms
+  C A0, K, O1, O3, O5, X, Y, Z;
+  if constexpr (NC) {
+    acc[0] = C(16) * ms2 - C(2) * ms1;
+    A0 = -ms1 - C(4) * ms2;
+    K = ms1 + ms2;
+    O1 = C(-4) * ms4;
+    O3 = C(-4) * ms6;
+    O5 = C(-4) * ms8;
+    X = ms4;
+    Y = ms6;
+    Z = ms8;
+  } else {
+    const C m0 = g[0] + Sa + Sd;
+    const C m3 = D1 + Xd, m5 = D3 + Yd, m7 = D5 + Zd;
+    const C ms0 = srate[0] * (m0 - meq_dev<D3Q15>(0, nd, compat));
+    const C ms3 = srate[3] * (m3 - meq_dev<D3Q15>(3, nd, compat));
+    const C ms5 = srate[5] * (m5 - meq_dev<D3Q15>(5, nd, compat));
+    const C ms7 = srate[7] * (m7 - meq_dev<D3Q15>(7, nd, compat));
+    acc[0] = ms0 - C(2) * ms1 + C(16) * ms2;
+    A0 = ms0 - ms1 - C(4) * ms2;
+    K = ms0 + ms1 + ms2;
+    O1 = ms3 - C(4) * ms4;
+    O3 = ms5 - C(4) * ms6;
+    O5 = ms7 - C(4) * ms8;
+    X = ms3 + ms4;
+    Y = ms5 + ms6;
+    Z = ms7 + ms8;
+  }
+  const C E1 = A0 + C(2) * ms9;
+  const C T = A0 - ms9;
+  const C E3 = T + ms10, E5 = T - ms10;
+  acc[1] = E1 + O1;
+  acc[2] = E1 - O1;
+  acc[3] = E3 + O3;
+  acc[4] = E3 - O3;
+  acc[5] = E5 + O5;
+  acc[6] = E5 - O5;
+  const C P = ms12 + ms13, R = ms12 - ms13;
+  const C Kp = K + ms11, Km = K - ms11;
+  const C E7 = Kp + P, E10 = Kp - P, E8 = Km + R, E9 = Km - R;
+  const C Zp = Z + ms14, Zm = Z - ms14, XY = X + Y, YX = Y - X;
+  const C O7 = Zp + XY, O10 = Zp - XY, O8 = Zm + YX, O9 = Zm - YX;
+  acc[7] = E7 + O7;
+  acc[14] = E7 - O7;
+  acc[8] = E8 + O8;
+  acc[13] = E8 - O8;
+  acc[9] = E9 + O9;
+  acc[12] = E9 - O9;
+  acc[10] = E10 + O10;
+  acc[11] = E10 - O10;
+}
+
 // The fluid-node collision of the reference (collision_functions[2 type +
 // forcing], LBM-C/collision.cu:19-421) after the macro/micro BCs
 // (LBM-C/solver.cu:111-112), written with opposite-pair symmetry: for a pair
@@ -504,8 +612,36 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
   C ft0e, ft0o;
   guo_parts(std::integral_constant<int, 0>{}, ft0e, ft0o);
 
-  if constexpr (COL == COL_MRT) {
-    // m* = S (M g - meq) / D; f <- f - M^T m* (collision.cu:192-303)
+  if constexpr ((COL == COL_MRT || COL == COL_MRT_NC) && L::Q == 15) {
+    // D3Q15 MRT (collision.cu:192-421) through the butterfly transforms.
+    C acc[15];
+    mrt_d3q15<C, COL == COL_MRT_NC>(nd, a.s_mrt, a.compat, acc);
+    if (a.compat & COMPAT_D3Q15_MINV_ZERO) {
+      // macros.cu:97-115: the reference's D3Q15 M_inv is all zeros.
+      unroll<Q>([&](auto kc) { acc[decltype(kc)::value] = 0; });
+    }
+    out[0] = nd.g[0] - omb * acc[0] + omb * ft0e;
+    const bool inplace = BLEND && (a.compat & COMPAT_MRTPOR_INPLACE);
+    unroll<L::NP>([&](auto pc) {
+      constexpr int i = L::pair(decltype(pc)::value);
+      constexpr int o = L::opp(i);
+      C fe, fo_;
+      guo_parts(std::integral_constant<int, i>{}, fe, fo_);
+      const C ft_i = fe + fo_, ft_o = fe - fo_;
+      if constexpr (BLEND) {
+        const C oi = nd.g[i] - omb * acc[i] + omb * ft_i + B * (nd.g[o] - nd.g[i]);
+        const C partner = inplace ? oi : nd.g[i];
+        out[i] = oi;
+        out[o] = nd.g[o] - omb * acc[o] + omb * ft_o + B * (partner - nd.g[o]);
+      } else {
+        out[i] = nd.g[i] - acc[i] + ft_i;
+        out[o] = nd.g[o] - acc[o] + ft_o;
+      }
+    });
+  } else if constexpr (COL == COL_MRT || COL == COL_MRT_NC) {
+    // m* = S (M g - meq) / D; f <- f - M^T m* (collision.cu:192-303).
+    // s_mrt holds s_k / D_k.  COL_MRT_NC drops the moments whose rate is
+    // zero (their m* is identically zero).
     C S[L::NP], D[L::NP];
     unroll<L::NP>([&](auto pc) {
       constexpr int p = decltype(pc)::value;
@@ -517,6 +653,10 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
     unroll<Q>([&](auto kc) {
       constexpr int k = decltype(kc)::value;
       constexpr bool even = moment_even<L>(k);
+      if constexpr (COL == COL_MRT_NC && moment_conserved<L>(k)) {
+        ms[k] = 0;
+        return;
+      }
       C mk = 0;
       if constexpr (even && L::m(k, 0) != 0) mk = C(L::m(k, 0)) * nd.g[0];
       unroll<L::NP>([&](auto pc) {
@@ -527,8 +667,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
         else if constexpr (c == -1) mk -= v;
         else if constexpr (c != 0) mk += C(c) * v;
       });
-      constexpr double inv_norm = 1.0 / (double)L::mnorm(k);
-      ms[k] = a.s_mrt[k] * (mk - meq_dev<L>(k, nd, a.compat)) * C(inv_norm);
+      ms[k] = a.s_mrt[k] * (mk - meq_dev<L>(k, nd, a.compat));
     });
     if (Q == 15 && (a.compat & COMPAT_D3Q15_MINV_ZERO)) {
       // macros.cu:97-115: the reference's D3Q15 M_inv is all zeros.
@@ -540,7 +679,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       unroll<Q>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
         constexpr int c = L::m(k, 0);
-        if constexpr (c != 0) acc += C(c) * ms[k];
+        if constexpr (c != 0 && !(COL == COL_MRT_NC && moment_conserved<L>(k))) acc += C(c) * ms[k];
       });
       out[0] = nd.g[0] - omb * acc + omb * ft0e;
     }
@@ -552,7 +691,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       unroll<Q>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
         constexpr int c = L::m(k, i);
-        if constexpr (c != 0) {
+        if constexpr (c != 0 && !(COL == COL_MRT_NC && moment_conserved<L>(k))) {
           if constexpr (moment_even<L>(k)) {
             if constexpr (c == 1) E += ms[k];
             else if constexpr (c == -1) E -= ms[k];
