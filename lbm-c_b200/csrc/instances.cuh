@@ -49,7 +49,7 @@ struct Launchers {
   // One block row per (y, z); blocks of up to STEP_BLOCK threads along x.
   static dim3 block_dim(const DeviceState &d) {
     int bx = (d.L[0] + 31) / 32 * 32;
-    return dim3(bx < STEP_BLOCK ? bx : STEP_BLOCK, 1, 1);
+    return dim3(bx < DIRECT_BLOCK ? bx : DIRECT_BLOCK, 1, 1);
   }
   static dim3 grid_dim(const DeviceState &d) {
     const int bx = (int)block_dim(d).x;
