@@ -38,7 +38,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "lbm-c_b200"))
 sys.path.insert(0, ROOT)
 
-METRIC = "GLUPS (D3Q15 MRT porous 256^3 fused step)"
 UNIT = "GLUPS"
 E2E_STEPS = 500
 STORAGE_BYTES = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}
@@ -159,30 +158,63 @@ def dist_barrier(world: int, device=None):
             dist.barrier()
 
 
+WORKLOAD_METRIC = {
+    "porous": "GLUPS (D3Q15 MRT porous {n}^3 fused step)",
+    "tgv": "GLUPS (D3Q15 BGK+Smagorinsky Taylor-Green {n}^3 fused step)",
+    "poiseuille": "GLUPS (D2Q9 BGK+Guo Poiseuille 128x64 fused step)",
+}
+
+
 def build_workload(args):
     import workloads
+    if args.workload == "tgv":
+        return workloads.taylor_green(args.size)
+    if args.workload == "poiseuille":
+        return workloads.poiseuille_channel()
     L = (args.size, args.size, args.size)
     return workloads.porous_spheres(L)
+
+
+def metric_name(args):
+    return WORKLOAD_METRIC[args.workload].format(n=args.size)
 
 
 # --------------------------------------------------------------- CPU legs
 
 class ReferenceTimer:
-    """The host-compiled reference step on a z-crop of the workload."""
+    """The host-compiled reference step on a crop (z, or y for 2-D) of the
+    workload."""
 
     def __init__(self, w, nz: int, threads: int):
         from oracle.oracle import Case, Reference
         lx, ly, lz = w.length
-        nz = max(1, min(nz, lz))
-        n = lx * ly * nz
+        if w.dim == 2:
+            ly_c, lz_c = ly, 1
+        else:
+            ly_c, lz_c = ly, max(1, min(nz, lz))
+        n = lx * ly_c * lz_c
         a = w.arrays
-        case = Case(lattice="d3q15", length=(lx, ly, nz), tau=w.tau, tau_mrt=w.tau_mrt,
-                    collision_type=w.collision_type, macro_bc=True, micro_bc=True,
-                    geometry=a["geometry"][:n], macro=a["macro"][:n], micro=a["micro"][:n],
-                    rho=a["rho"][:n], u=a["u"][:, :n])
-        self.ref = Reference(case, "patched", nthreads=threads)
+
+        def crop(x, comp=False):
+            if x is None:
+                return None
+            return x[:, :n] if comp else x[:n]
+        f0 = None
+        if w.init_type == 1:  # f_eq(rho, u), as lbmc_init does
+            from oracle.oracle import Restatement
+            tmp = Case(lattice=w.lattice, length=(lx, ly_c, lz_c))
+            f0 = Restatement(tmp).equilibrium(crop(a["rho"]), crop(a["u"], True))
+        case = Case(lattice=w.lattice, length=(lx, ly_c, lz_c), tau=w.tau, tau_mrt=w.tau_mrt,
+                    c_smag=w.c_smag, collision_type=w.collision_type, forcing=w.forcing,
+                    macro_bc=w.macro_bc, micro_bc=w.micro_bc,
+                    geometry=crop(a.get("geometry")), force=crop(a.get("force"), True),
+                    macro=crop(a.get("macro")), micro=crop(a.get("micro")),
+                    rho=crop(a.get("rho")), u=crop(a.get("u"), True), f0=f0)
+        variant = "patched" if (w.lattice == "d3q15" or w.c_smag > 0) else "asis"
+        self.ref = Reference(case, variant, nthreads=threads)
         self.n, self.threads = n, threads
-        self.sample = f"{lx}x{ly}x{nz} z-crop of the workload, FP64, patched reference step"
+        shape = f"{lx}x{ly_c}" if w.dim == 2 else f"{lx}x{ly_c}x{lz_c}"
+        self.sample = f"{shape} crop of the workload, FP64, {variant} reference step"
 
     def rate(self, steps: int) -> float:
         """Lattice updates per second over `steps` reference steps."""
@@ -224,12 +256,12 @@ def run_reference_arm(args, world, rank):
     timer.close()
     value = timer.n * steps / t_total / 1e9
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded sphere pack)", "impl": "reference",
-        "config": {"workload": f"porous_spheres_d3q15_mrt_{args.size}^3",
-                   "sample": timer.sample, "storage": "f64", "l2": "inputs larger than L2"},
+        "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": w.name, "nodes": w.n, "sample": timer.sample, "storage": "f64",
+                   "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{timer.sample}, {steps} steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -279,9 +311,9 @@ def run_ours(args, world, rank, local):
     per_launch_s = (ms / 1e3) / args.steps
     achieved = w.n * bpl / per_launch_s / 1e9
     peak, peak_kind = measured_peak()
-    tag = f"step_kernel_porous{args.size}_{args.storage}"
-    if args.kernel != "direct":
-        tag = f"step_pipelined_kernel_porous{args.size}_{args.storage}"
+    tag = f"step_kernel_{args.workload}{args.size}_{args.storage}"
+    if args.kernel == "pipelined":
+        tag = f"step_pipelined_kernel_{args.workload}{args.size}_{args.storage}"
     traffic = profiled_traffic(tag)
 
     # End to end through the C ABI with host buffers.
@@ -315,20 +347,24 @@ def run_ours(args, world, rank, local):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": args.storage, "data": "synthetic (seeded sphere pack)",
-            "config": {"workload": f"porous_spheres_d3q15_mrt_{args.size}^3",
-                       "nodes": w.n, "storage": args.storage, "compute": "f32" if args.storage != "f64" else "f64",
-                       "solid_fraction": round(w.params["solid_fraction"], 4),
-                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)"},
+            "dtype": args.storage, "data": "synthetic (seeded)",
+            "config": {"workload": w.name, "length": list(w.length), "nodes": w.n,
+                       "storage": args.storage,
+                       "compute": "f32" if args.storage != "f64" else "f64",
+                       "params": {k: (round(v, 6) if isinstance(v, float) else v)
+                                  for k, v in w.params.items()},
+                       "parallelism": f"replicas{world}",
+                       "l2": ("inputs larger than L2 (no flush)" if w.n * w.q * 2 > 126e6
+                              else "inputs fit in L2: steady-state in-cache rate")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
                          "bytes_per_lup": bpl,
                          "kernel": ("step_pipelined_kernel (bulk-copy row pipeline, fused stream+BC+collide)"
-                                    if args.kernel != "direct" else
+                                    if args.kernel == "pipelined" else
                                     "step_kernel (direct loads, fused stream+BC+collide)")},
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -349,6 +385,7 @@ def main():
     ap.add_argument("--storage", choices=list(STORAGE_BYTES), default="f32")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--kernel", choices=["auto", "direct", "pipelined"], default="auto")
+    ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
