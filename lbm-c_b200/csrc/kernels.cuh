@@ -45,15 +45,19 @@ __device__ __forceinline__ void unroll(F &&f) {
 template <class S>
 struct Storage;
 
-// Population stores use the streaming (evict-first) cache hint: every slot
-// is written once per step and next read one step later, after the whole
-// 0.5-8 GB population set has streamed through the 126 MB L2.
+// Storage formats.  put() writes a population to global memory with the
+// streaming (evict-first) cache hint: every slot is written once per step and
+// next read one step later, after the whole population set has streamed
+// through the 126 MB L2.  put_any() is a plain store for pointers that may be
+// in shared memory (the bulk-copy pipeline's stages); the .cs hint is a
+// global-space instruction and must never see a shared-memory address.
 template <>
 struct Storage<double> {
   using C = double;
   static constexpr bool SCALED = false;
   static __device__ __forceinline__ C get(const double *p) { return *p; }
   static __device__ __forceinline__ void put(double *p, C v) { __stcs(p, v); }
+  static __device__ __forceinline__ void put_any(double *p, C v) { *p = v; }
 };
 template <>
 struct Storage<float> {
@@ -61,6 +65,7 @@ struct Storage<float> {
   static constexpr bool SCALED = false;
   static __device__ __forceinline__ C get(const float *p) { return *p; }
   static __device__ __forceinline__ void put(float *p, C v) { __stcs(p, v); }
+  static __device__ __forceinline__ void put_any(float *p, C v) { *p = v; }
 };
 // FP16 keeps (f - w) * scale so that small deviations stay out of the
 // subnormal range; BF16 has FP32's exponent range and needs no scale.
@@ -70,6 +75,7 @@ struct Storage<__half> {
   static constexpr bool SCALED = true;
   static __device__ __forceinline__ C get(const __half *p) { return __half2float(*p); }
   static __device__ __forceinline__ void put(__half *p, C v) { __stcs(p, __float2half_rn(v)); }
+  static __device__ __forceinline__ void put_any(__half *p, C v) { *p = __float2half_rn(v); }
 };
 template <>
 struct Storage<__nv_bfloat16> {
@@ -77,6 +83,7 @@ struct Storage<__nv_bfloat16> {
   static constexpr bool SCALED = false;
   static __device__ __forceinline__ C get(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
   static __device__ __forceinline__ void put(__nv_bfloat16 *p, C v) { __stcs(p, __float2bfloat16_rn(v)); }
+  static __device__ __forceinline__ void put_any(__nv_bfloat16 *p, C v) { *p = __float2bfloat16_rn(v); }
 };
 
 // Stored-value conversions with the storage scale applied only where the
@@ -86,10 +93,17 @@ __device__ __forceinline__ typename Storage<S>::C load_dev(const S *p, typename 
   if constexpr (Storage<S>::SCALED) return Storage<S>::get(p) * inv_scale;
   else return Storage<S>::get(p);
 }
+// Global-memory population store (streaming hint).
 template <class S>
 __device__ __forceinline__ void store_dev(S *p, typename Storage<S>::C v, typename Storage<S>::C scale) {
   if constexpr (Storage<S>::SCALED) Storage<S>::put(p, v * scale);
   else Storage<S>::put(p, v);
+}
+// Shared-memory (or generic) population store, no cache hint.
+template <class S>
+__device__ __forceinline__ void store_smem(S *p, typename Storage<S>::C v, typename Storage<S>::C scale) {
+  if constexpr (Storage<S>::SCALED) Storage<S>::put_any(p, v * scale);
+  else Storage<S>::put_any(p, v);
 }
 
 // ------------------------------------------------------------ node classes
@@ -855,9 +869,16 @@ __device__ __forceinline__ void block_diag(const double (&v)[DIAG_VALUES], bool 
 // Fallback for rows whose byte length is not a multiple of 16 (bulk copies
 // need 16-byte granules) or that do not fit the shared-memory stages.
 // Grid: blockDim (bx, 1, 1) along x, gridDim (ceil(Lx/bx), Ly, Lz).
+template <class S, int COL>
+constexpr int direct_min_blocks() {
+  // FP64 arithmetic needs register pairs: no cap beyond the 128 per thread
+  // that 8 resident blocks imply.
+  if (std::is_same<S, double>::value) return 8;
+  return COL == COL_BGK_SMAG ? DIRECT_MIN_BLOCKS_SMAG : DIRECT_MIN_BLOCKS;
+}
+
 template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG>
-__global__ void __launch_bounds__(DIRECT_BLOCK, COL == COL_BGK_SMAG ? DIRECT_MIN_BLOCKS_SMAG
-                                                                    : DIRECT_MIN_BLOCKS)
+__global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
     step_kernel(const StepArgs<typename Storage<S>::C> a) {
   using C = typename Storage<S>::C;
   constexpr int Q = L::Q;
@@ -1130,7 +1151,7 @@ __global__ void __launch_bounds__(STEP_BLOCK + 32)
           constexpr int i = decltype(ic)::value;
           constexpr int ex = L::e(0, i);
           const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
-          store_dev(sb + i * lx + xs, out[i], scale);
+          store_smem(sb + i * lx + xs, out[i], scale);
         });
         store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
       }
