@@ -215,6 +215,24 @@ const char *lbmc_status_string(lbmc_status s);
  * reference, which has no device-side waits. */
 lbmc_status lbmc_selftest_wait_timeout(int device, double seconds);
 
+/* FP64 sums of rho, rho*u and 0.5*rho*|u|^2 (the lbmc_diag quantities) over
+ * n nodes of caller-owned device arrays, written to sums[0..4] (device
+ * memory: mass, momentum x/y/z, kinetic energy), ordered on cuda_stream
+ * (NULL = legacy default stream).  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory when they need the sums
+ * (an application whose own pool allocator already holds the device memory,
+ * a process under a device-memory cap, a time loop that must avoid
+ * cudaMalloc's implicit synchronisation).  It allocates nothing: its
+ * per-block scratch is a fixed 320 KiB array in the library's device image,
+ * so n is limited to 134,217,728 nodes (512^3); larger n, NULL rho/ux/sums
+ * or n < 1 return LBMC_ERR_INVALID_ARG.  uy/uz may be NULL (zero).  The
+ * first call on a device looks up the scratch array's address (make it
+ * before any stream capture).  Calls share the scratch: calls whose kernels
+ * overlap on the GPU race; stream-ordered calls do not. */
+lbmc_status lbmc_macro_sums_noalloc(int device, const double *rho, const double *ux,
+                                    const double *uy, const double *uz, long long n,
+                                    double *sums, void *cuda_stream);
+
 /* Host-only helpers (no GPU needed). */
 
 /* Checks a configuration and domain the way lbmc_init does, without touching

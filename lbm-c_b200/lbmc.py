@@ -103,6 +103,9 @@ def library() -> ctypes.CDLL:
         lib.lbmc_lattice_tables.argtypes = [ctypes.c_int, _P, _P, _P, _P]
         lib.lbmc_selftest_wait_timeout.argtypes = [ctypes.c_int, ctypes.c_double]
         lib.lbmc_selftest_wait_timeout.restype = ctypes.c_int
+        lib.lbmc_macro_sums_noalloc.argtypes = [ctypes.c_int, _P, _P, _P, _P, ctypes.c_longlong,
+                                                _P, _P]
+        lib.lbmc_macro_sums_noalloc.restype = ctypes.c_int
         for name in ("lbmc_config_default", "lbmc_validate", "lbmc_init", "lbmc_iterate",
                      "lbmc_fetch", "lbmc_destroy", "lbmc_get_step", "lbmc_set_stream",
                      "lbmc_synchronize", "lbmc_classify", "lbmc_lattice_tables"):
