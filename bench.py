@@ -149,6 +149,24 @@ def dist_max(value: float, world: int, device=None) -> float:
     return float(t.item())
 
 
+def dist_sum(value: float, world: int, device=None) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def aggregate_rate(units_local: float, seconds_local: float, world: int, device=None):
+    """Whole-job throughput of independent replicas: all ranks' units over the
+    slowest rank's time.  Returns (units per second, max seconds)."""
+    t_max = dist_max(seconds_local, world, device)
+    units = dist_sum(units_local, world, device)
+    return units / t_max, t_max
+
+
 def dist_barrier(world: int, device=None):
     if world > 1:
         import torch.distributed as dist
@@ -298,9 +316,9 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize(device)
     dist_barrier(world, device)
     ms = start.elapsed_time(stop)
-    ms_max = dist_max(ms, world, device)
-    lups = w.n * args.steps * world
-    value = lups / (ms_max / 1e3) / 1e9
+    rate, t_max = aggregate_rate(w.n * args.steps, ms / 1e3, world, device)
+    ms_max = t_max * 1e3
+    value = rate / 1e9
     eng.iterate(1, lbmc.REDUCE_DIAG | lbmc.SYNC)
     diag = eng.diag()
     eng.close()
@@ -333,8 +351,8 @@ def run_ours(args, world, rank, local):
             dt = time.perf_counter() - t
             if k > 0:
                 times.append(dt)
-        t_e2e = dist_max(max(times), world, device)
-        e2e = {"value": w.n * E2E_STEPS * world / t_e2e / 1e9, "unit": UNIT,
+        e2e_rate, _ = aggregate_rate(w.n * E2E_STEPS, max(times), world, device)
+        e2e = {"value": e2e_rate / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "job": f"lbmc_init from host arrays + {E2E_STEPS} steps + fetch rho,u + destroy"}
 

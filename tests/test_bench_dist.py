@@ -1,0 +1,55 @@
+"""bench.py's multi-rank path (independent replicas) on CPU with gloo,
+world_size 2: the barrier and the whole-job aggregation (all ranks' units
+over the slowest rank's time) agree on every rank."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, q):
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+
+    import bench
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        bench.dist_barrier(world)
+        rate, t_max = bench.aggregate_rate(100.0 * (rank + 1), 1.0 + rank, world)
+        q.put((rank, rate, t_max))
+        bench.dist_barrier(world)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replica_aggregation_gloo_world2():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    for rank, rate, t_max in got:
+        assert t_max == pytest.approx(2.0)
+        assert rate == pytest.approx(300.0 / 2.0)
+
+
+def test_single_rank_aggregation_is_local():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.aggregate_rate(50.0, 2.0, 1) == (25.0, 2.0)
