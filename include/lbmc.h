@@ -233,6 +233,51 @@ lbmc_status lbmc_macro_sums_noalloc(int device, const double *rho, const double 
                                     const double *uy, const double *uz, long long n,
                                     double *sums, void *cuda_stream);
 
+/* ---------------- batched small domains (no reference counterpart) -------
+ * Thousands of independent D2Q9 domains with the same physics (BGK or
+ * NTPOR + uniform Guo force, Init 0) stepped by one persistent kernel
+ * replayed from a CUDA graph until every domain's max |u(t) - u(t-1)| falls
+ * below a tolerance.  Each domain evolves exactly as one lbmc handle would. */
+typedef struct lbmc_batch lbmc_batch;
+
+typedef struct lbmc_batch_config {
+  double tau;
+  double force[2];      /* uniform Guo body force */
+  int collision_type;   /* LBMC_BGK or LBMC_NTPOR */
+  int storage;          /* LBMC_F32, LBMC_F16 or LBMC_BF16 */
+  double storage_scale; /* 0 = default (1024 for FP16) */
+  int device;
+  int block_threads;    /* 0 = autotune (256/512/1024) */
+  int steps_per_launch; /* 0 = autotune (check_every or 4*check_every) */
+  int reserved[8];
+} lbmc_batch_config;
+
+typedef struct lbmc_batch_domain {
+  int length[2];            /* Lx, Ly */
+  const double *geometry;   /* Lx*Ly Porosity B: 0 fluid, (0,1) partial, >= 1 solid; NULL = fluid */
+} lbmc_batch_domain;
+
+typedef struct lbmc_batch_result {
+  long long steps;    /* steps run */
+  double delta_u;     /* last max |u(t) - u(t-1)| measured */
+  double elapsed_ms;  /* device time from the run's start to convergence, -1 if not converged */
+  int converged;      /* 1 if delta_u < tol was reached before the step cap */
+  int reserved;
+} lbmc_batch_result;
+
+lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomains,
+                            const lbmc_batch_domain *doms, lbmc_batch **out);
+/* Runs until every domain converged (delta_u < tol, checked every
+ * check_every steps) or reached max_steps; results has ndomains entries. */
+lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double tol, int check_every,
+                           lbmc_batch_result *results);
+/* LBMC_FIELD_RHO / U_X / U_Y (N doubles; u = j/rho) or LBMC_FIELD_F (9N). */
+lbmc_status lbmc_batch_fetch(lbmc_batch *b, int domain, int field, void *dst, size_t bytes);
+/* Launch shape chosen by the autotuner and how many domains stay in shared memory. */
+lbmc_status lbmc_batch_info(lbmc_batch *b, long long *total_nodes, int *threads,
+                            int *steps_per_launch, int *resident_domains);
+lbmc_status lbmc_batch_destroy(lbmc_batch *b);
+
 /* Host-only helpers (no GPU needed). */
 
 /* Checks a configuration and domain the way lbmc_init does, without touching

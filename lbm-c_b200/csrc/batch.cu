@@ -1,0 +1,590 @@
+// Batched persistent step for many independent small D2Q9 domains
+// (lbmc_batch_*).  No counterpart in the reference, which runs one domain per
+// process; each domain here is stepped exactly as lbmc_iterate steps a single
+// domain (same shift layout, same collide_fluid), so parity is inherited.
+//
+// Execution model.  One persistent kernel launch advances every unconverged
+// domain by up to K steps.  Blocks take domains from an atomic queue (domains
+// sorted by size, largest first); a whole domain belongs to one block, so the
+// step-to-step dependency is a __syncthreads, not a grid barrier.  A domain
+// whose populations fit in the block's shared memory is loaded once, stepped
+// K times in shared memory and written back, so its K steps cost one read and
+// one write of HBM; larger domains are stepped in HBM.  Every C steps a
+// domain compares u with the previous step (max norm) and freezes once below
+// the tolerance, recording the device timer.  The host replays a CUDA graph
+// (queue reset + kernel) until all domains converged or hit the step cap.  An
+// autotuner times the first launches with several block sizes and K, keeps
+// the fastest.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/lbmc.h"
+#include "engine_internal.h"
+#include "kernels.cuh"
+
+using namespace lbmc;
+
+namespace {
+
+struct BatchDomainDev {
+  long long pop_off;   // element offset of population 0 in the pool
+  long long node_off;  // offset into class / porosity / u_prev arrays
+  int pitch;           // elements between populations (global)
+  int lx, ly;
+  int resident;        // fits in shared memory
+};
+
+struct BatchStateDev {
+  long long t;                  // steps done
+  float delta_u;                // last max |u(t) - u(t-1)|
+  int converged;                // 1 converged, 2 stopped at the step cap
+  unsigned long long done_ns;   // device timer at convergence
+};
+
+struct BatchArgs {
+  void *pool;
+  const uint8_t *cls;
+  const float *B;
+  float2 *u_prev;
+  const BatchDomainDev *dom;
+  BatchStateDev *state;
+  const int *order;          // domains, largest first
+  int ndomains;
+  int *queue;                // atomic work counter (reset before each launch)
+  int *active;               // domains still running after this launch
+  int steps;                 // K: steps per launch per domain
+  int check;                 // C: convergence check interval
+  float tol;
+  long long max_steps;
+  float tau, force[2];
+  float scale, inv_scale;
+  int blend;
+  size_t smem_elems;         // capacity of the shared-memory population buffer
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// One D2Q9 node: load its 9 shift slots from `pop` (pitch elements apart),
+// collide, write back; returns u = j/rho + F/(2 rho) in `u` (the stored
+// velocity of LBM-C/collision.cu:77).
+template <class S, bool BLEND>
+__device__ __forceinline__ void batch_node(S *pop, long long pitch, int k, int x, int y, int lx, int ly,
+                                           int sx, int sy, int cls, const StepArgs<float> &a,
+                                           float &ux, float &uy) {
+  using L = D2Q9;
+  const int xs[3] = {x, wrap_sub(x, sx, lx), wrap_add(x, sx, lx)};
+  const int ys[3] = {y, wrap_sub(y, sy, ly), wrap_add(y, sy, ly)};
+  Node<L, float> nd;
+  unroll<9>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const int slot = xs[sel(L::e(0, i))] + lx * ys[sel(L::e(1, i))];
+    nd.g[i] = load_dev(pop + i * pitch + slot, a.inv_scale);
+  });
+  float out[9];
+  if (cls == CLASS_SOLID) {
+    collide_solid(nd, out);
+  } else {
+    moments(nd);
+    // a.B is this domain's porosity array; only partial nodes read it.
+    collide_fluid<L, float, COL_BGK, true, BLEND>(nd, a, k, cls == 2 ? ENTRY_PARTIAL : 0u, out);
+  }
+  unroll<9>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    const int slot = xs[sel(L::e(0, i))] + lx * ys[sel(L::e(1, i))];
+    store_smem(pop + i * pitch + slot, out[i], a.scale);
+  });
+  ux = nd.u[0];
+  uy = nd.u[1];
+}
+
+__device__ __forceinline__ float block_max(float v, float *sh) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  float r = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = fmaxf(r, sh[w]);
+  return r;
+}
+
+template <class S, bool BLEND>
+__global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int sh_dom;
+  __shared__ float sh_red[32];
+  __shared__ int sh_stop;
+  S *sbuf = reinterpret_cast<S *>(smem_raw);
+  S *pool = reinterpret_cast<S *>(A.pool);
+  StepArgs<float> a;
+  memset(&a, 0, sizeof(a));
+  a.tau = A.tau;
+  a.force_u[0] = A.force[0];
+  a.force_u[1] = A.force[1];
+  a.scale = A.scale;
+  a.inv_scale = A.inv_scale;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int q = atomicAdd(A.queue, 1);
+      sh_dom = q < A.ndomains ? A.order[q] : -1;
+    }
+    __syncthreads();
+    const int d = sh_dom;
+    __syncthreads();
+    if (d < 0) break;
+    BatchStateDev &st = A.state[d];
+    if (st.converged) continue;
+    const BatchDomainDev D = A.dom[d];
+    const int n = D.lx * D.ly;
+    const uint8_t *cls = A.cls + D.node_off;
+    a.B = A.B + D.node_off;
+    float2 *up = A.u_prev + D.node_off;
+    S *pop = pool + D.pop_off;
+    long long pitch = D.pitch;
+    if (D.resident) {
+      for (int i = 0; i < 9; i++)
+        for (int k = threadIdx.x; k < n; k += blockDim.x) sbuf[(long long)i * n + k] = pop[(long long)i * D.pitch + k];
+      pop = sbuf;
+      pitch = n;
+      __syncthreads();
+    }
+    long long t = st.t;
+    int stop = 0;
+    for (int s = 0; s < A.steps && !stop; s++, t++) {
+      const int sx = (int)(t % D.lx), sy = (int)(t % D.ly);
+      const bool save = ((t + 1) % A.check) == 0;
+      const bool test = t > 0 && (t % A.check) == 0;
+      float dmax = 0;
+      for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int x = k % D.lx, y = k / D.lx;
+        const int c = cls[k];
+        float ux, uy;
+        batch_node<S, BLEND>(pop, pitch, k, x, y, D.lx, D.ly, sx, sy, c, a, ux, uy);
+        if (test) {
+          const float2 p = up[k];
+          dmax = fmaxf(dmax, fmaxf(fabsf(ux - p.x), fabsf(uy - p.y)));
+        }
+        if (save) up[k] = make_float2(ux, uy);
+      }
+      __syncthreads();
+      if (test) {
+        const float m = block_max(dmax, sh_red);
+        if (threadIdx.x == 0) {
+          st.delta_u = m;
+          sh_stop = m < A.tol ? 1 : 0;
+        }
+        __syncthreads();
+        stop = sh_stop;
+      }
+      if (t + 1 >= A.max_steps) stop = stop ? stop : 2;
+    }
+    if (D.resident) {
+      __syncthreads();
+      for (int i = 0; i < 9; i++)
+        for (int k = threadIdx.x; k < n; k += blockDim.x)
+          Storage<S>::put_any(pool + D.pop_off + (long long)i * D.pitch + k, Storage<S>::get(sbuf + (long long)i * n + k));
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      st.t = t;
+      if (stop) {
+        st.converged = stop;
+        st.done_ns = global_ns();
+      } else {
+        atomicAdd(A.active, 1);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void stamp_kernel(unsigned long long *out) { *out = global_ns(); }
+
+}  // namespace
+
+struct lbmc_batch {
+  lbmc_batch_config cfg;
+  int ndomains = 0;
+  std::vector<BatchDomainDev> dom;
+  std::vector<int> order;
+  void *pool = nullptr;
+  uint8_t *cls = nullptr;
+  float *B = nullptr;
+  float2 *u_prev = nullptr;
+  BatchDomainDev *dom_dev = nullptr;
+  BatchStateDev *state = nullptr;
+  int *order_dev = nullptr;
+  int *counters = nullptr;  // [0] queue, [1] active
+  unsigned long long *t0 = nullptr;
+  cudaStream_t stream = nullptr;
+  int ssize = 4;
+  bool blend = false;
+  long long total_nodes = 0;
+  size_t smem_bytes = 0;
+  int sms = 0;
+  int threads = 0, steps = 0;  // tuned launch shape
+  double scale = 1;
+};
+
+namespace {
+
+lbmc_status berr(lbmc_status s, const std::string &m) {
+  lbmc::set_last_error(m);
+  return s;
+}
+
+template <class S>
+cudaError_t configure_batch(lbmc_batch *b) {
+  cudaError_t e = cudaFuncSetAttribute(batch_kernel<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)b->smem_bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(batch_kernel<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)b->smem_bytes);
+  return e;
+}
+
+template <class S>
+cudaError_t launch_batch(lbmc_batch *b, const BatchArgs &A, int threads, cudaStream_t st) {
+  auto kern = b->blend ? batch_kernel<S, true> : batch_kernel<S, false>;
+  kern<<<b->sms, threads, b->smem_bytes, st>>>(A);
+  return cudaGetLastError();
+}
+
+BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long max_steps) {
+  BatchArgs A;
+  memset(&A, 0, sizeof(A));
+  A.pool = b->pool;
+  A.cls = b->cls;
+  A.B = b->B;
+  A.u_prev = b->u_prev;
+  A.dom = b->dom_dev;
+  A.state = b->state;
+  A.order = b->order_dev;
+  A.ndomains = b->ndomains;
+  A.queue = b->counters;
+  A.active = b->counters + 1;
+  A.steps = steps;
+  A.check = check;
+  A.tol = (float)tol;
+  A.max_steps = max_steps;
+  A.tau = (float)b->cfg.tau;
+  A.force[0] = (float)b->cfg.force[0];
+  A.force[1] = (float)b->cfg.force[1];
+  A.scale = (float)b->scale;
+  A.inv_scale = (float)(1.0 / b->scale);
+  A.blend = b->blend;
+  A.smem_elems = b->smem_bytes / b->ssize;
+  return A;
+}
+
+cudaError_t enqueue(lbmc_batch *b, const BatchArgs &A, int threads, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, 2 * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  switch (b->cfg.storage) {
+    case LBMC_F16: return launch_batch<__half>(b, A, threads, st);
+    case LBMC_BF16: return launch_batch<__nv_bfloat16>(b, A, threads, st);
+    default: return launch_batch<float>(b, A, threads, st);
+  }
+}
+
+}  // namespace
+
+extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomains,
+                                       const lbmc_batch_domain *doms, lbmc_batch **out) {
+  if (!cfg || !doms || !out || ndomains < 1) return berr(LBMC_ERR_INVALID_ARG, "lbmc_batch_init: NULL or empty");
+  *out = nullptr;
+  if (!(cfg->tau > 0.5) || !std::isfinite(cfg->tau)) return berr(LBMC_ERR_INVALID_ARG, "tau must be > 0.5");
+  if (cfg->collision_type != LBMC_BGK && cfg->collision_type != LBMC_NTPOR)
+    return berr(LBMC_ERR_UNSUPPORTED, "batched domains support ColType BGK and NTPOR");
+  if (cfg->storage != LBMC_F32 && cfg->storage != LBMC_F16 && cfg->storage != LBMC_BF16)
+    return berr(LBMC_ERR_UNSUPPORTED, "batched domains store FP32, FP16 or BF16");
+  if (cudaSetDevice(cfg->device) != cudaSuccess) {
+    cudaGetLastError();
+    return berr(LBMC_ERR_NO_DEVICE, "no such device");
+  }
+  lbmc_batch *b = new lbmc_batch();
+  b->cfg = *cfg;
+  b->ndomains = ndomains;
+  b->ssize = cfg->storage == LBMC_F32 ? 4 : 2;
+  b->scale = cfg->storage_scale > 0 ? cfg->storage_scale : (cfg->storage == LBMC_F16 ? 1024.0 : 1.0);
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, cfg->device);
+  int smem_optin = 0;
+  cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, cfg->device);
+  b->smem_bytes = (size_t)std::max(0, smem_optin - 2048);  // leave room for static shared memory
+  const size_t resident_elems = b->smem_bytes / b->ssize;
+
+  // Layout: populations padded to 64 elements per array (128-byte aligned).
+  long long pop = 0, node = 0;
+  b->dom.resize(ndomains);
+  for (int d = 0; d < ndomains; d++) {
+    const int lx = doms[d].length[0], ly = doms[d].length[1];
+    if (lx < 1 || ly < 1 || (long long)lx * ly > (1LL << 30)) {
+      delete b;
+      return berr(LBMC_ERR_INVALID_ARG, "domain " + std::to_string(d) + " has a bad size");
+    }
+    const long long n = (long long)lx * ly;
+    BatchDomainDev &D = b->dom[d];
+    D.lx = lx;
+    D.ly = ly;
+    D.pitch = (int)((n + 63) / 64 * 64);
+    D.pop_off = pop;
+    D.node_off = node;
+    D.resident = (size_t)n * 9 <= resident_elems;
+    pop += 9LL * D.pitch;
+    node += n;
+  }
+  b->total_nodes = node;
+  std::vector<uint8_t> cls(node, 0);
+  std::vector<float> B(node, 0.f);
+  for (int d = 0; d < ndomains; d++) {
+    const long long n = (long long)b->dom[d].lx * b->dom[d].ly;
+    for (long long k = 0; k < n; k++) {
+      const double v = doms[d].geometry ? doms[d].geometry[k] : 0.0;
+      if (!std::isfinite(v)) {
+        delete b;
+        return berr(LBMC_ERR_INVALID_ARG, "non-finite porosity");
+      }
+      uint8_t c = 0;
+      if (v >= 1) c = CLASS_SOLID;
+      else if (v != 0 && cfg->collision_type == LBMC_NTPOR) c = 2;
+      cls[b->dom[d].node_off + k] = c;
+      B[b->dom[d].node_off + k] = (float)v;
+      if (c == 2) b->blend = true;
+    }
+  }
+  b->order.resize(ndomains);
+  std::iota(b->order.begin(), b->order.end(), 0);
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+    return (long long)b->dom[x].lx * b->dom[x].ly > (long long)b->dom[y].lx * b->dom[y].ly;
+  });
+  cudaError_t e = cudaSuccess;
+  auto alloc = [&](void **p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes ? bytes : 16);
+  };
+  alloc(&b->pool, (size_t)pop * b->ssize);
+  alloc((void **)&b->cls, node);
+  alloc((void **)&b->B, node * sizeof(float));
+  alloc((void **)&b->u_prev, node * sizeof(float2));
+  alloc((void **)&b->dom_dev, ndomains * sizeof(BatchDomainDev));
+  alloc((void **)&b->state, ndomains * sizeof(BatchStateDev));
+  alloc((void **)&b->order_dev, ndomains * sizeof(int));
+  alloc((void **)&b->counters, 2 * sizeof(int));
+  alloc((void **)&b->t0, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(b->pool, 0, (size_t)pop * b->ssize);  // f = w (Init 0)
+  if (e == cudaSuccess) e = cudaMemcpy(b->cls, cls.data(), node, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->B, B.data(), node * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(b->u_prev, 0, node * sizeof(float2));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->dom_dev, b->dom.data(), ndomains * sizeof(BatchDomainDev), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(b->state, 0, ndomains * sizeof(BatchStateDev));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->order_dev, b->order.data(), ndomains * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    switch (cfg->storage) {
+      case LBMC_F16: e = configure_batch<__half>(b); break;
+      case LBMC_BF16: e = configure_batch<__nv_bfloat16>(b); break;
+      default: e = configure_batch<float>(b); break;
+    }
+  }
+  if (e != cudaSuccess) {
+    lbmc_batch_destroy(b);
+    return berr(e == cudaErrorMemoryAllocation ? LBMC_ERR_ALLOC : LBMC_ERR_CUDA,
+                std::string("lbmc_batch_init: ") + cudaGetErrorString(e));
+  }
+  b->threads = cfg->block_threads;
+  b->steps = cfg->steps_per_launch;
+  *out = b;
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double tol, int check_every,
+                                      lbmc_batch_result *results) {
+  if (!b || max_steps < 1 || check_every < 1 || !(tol >= 0))
+    return berr(LBMC_ERR_INVALID_ARG, "lbmc_batch_run: bad arguments");
+  if (cudaSetDevice(b->cfg.device) != cudaSuccess) return berr(LBMC_ERR_CUDA, "cudaSetDevice");
+  cudaError_t e = cudaSuccess;
+  stamp_kernel<<<1, 1, 0, b->stream>>>(b->t0);
+
+  // Autotune the launch shape on the first launches (they are real steps).
+  if (b->threads <= 0 || b->steps <= 0) {
+    const int cand_threads[3] = {256, 512, 1024};
+    const int cand_steps[2] = {check_every, 4 * check_every};
+    double best = -1;
+    int bt = 512, bs = check_every;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int ti = 0; ti < 3; ti++)
+      for (int si = 0; si < 2; si++) {
+        const int th = b->threads > 0 ? b->threads : cand_threads[ti];
+        const int sp = b->steps > 0 ? b->steps : cand_steps[si];
+        const BatchArgs A = make_args(b, sp, check_every, tol, max_steps);
+        cudaEventRecord(e0, b->stream);
+        e = enqueue(b, A, th, b->stream);
+        cudaEventRecord(e1, b->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) break;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double rate = (double)sp / ms;  // steps per ms over the whole batch
+        if (rate > best) {
+          best = rate;
+          bt = th;
+          bs = sp;
+        }
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    b->threads = bt;
+    b->steps = bs;
+  }
+
+  // Capture one launch (queue reset + kernel) in a graph and replay it.
+  const BatchArgs A = make_args(b, b->steps, check_every, tol, max_steps);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t e2 = enqueue(b, A, b->threads, b->stream);
+    e = cudaStreamEndCapture(b->stream, &graph);
+    if (e2 != cudaSuccess) e = e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  int active = 1;
+  const long long launches_max = max_steps / std::max(1, b->steps) + 2;
+  for (long long l = 0; e == cudaSuccess && active > 0 && l < launches_max; l++) {
+    e = cudaGraphLaunch(exec, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&active, b->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
+  if (results) {
+    std::vector<BatchStateDev> st(b->ndomains);
+    unsigned long long t0 = 0;
+    e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&t0, b->t0, sizeof(t0), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, cudaGetErrorString(e));
+    for (int d = 0; d < b->ndomains; d++) {
+      results[d].steps = st[d].t;
+      results[d].delta_u = st[d].delta_u;
+      results[d].converged = st[d].converged == 1;
+      results[d].elapsed_ms = st[d].converged ? (double)(st[d].done_ns - t0) * 1e-6 : -1.0;
+    }
+  }
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_batch_info(lbmc_batch *b, long long *total_nodes, int *threads,
+                                       int *steps_per_launch, int *resident_domains) {
+  if (!b) return berr(LBMC_ERR_INVALID_ARG, "NULL batch");
+  if (total_nodes) *total_nodes = b->total_nodes;
+  if (threads) *threads = b->threads;
+  if (steps_per_launch) *steps_per_launch = b->steps;
+  if (resident_domains) {
+    int r = 0;
+    for (const auto &D : b->dom) r += D.resident;
+    *resident_domains = r;
+  }
+  return LBMC_OK;
+}
+
+namespace {
+
+template <class S>
+__global__ void batch_fetch_kernel(const S *pop, long long pitch, int lx, int ly, long long t, float inv_scale,
+                                   double *rho, double *ux, double *uy, double *f) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= lx * ly) return;
+  using L = D2Q9;
+  const int x = k % lx, y = k / lx;
+  const int sx = (int)(t % lx), sy = (int)(t % ly);
+  const int xs[3] = {x, wrap_sub(x, sx, lx), wrap_add(x, sx, lx)};
+  const int ys[3] = {y, wrap_sub(y, sy, ly), wrap_add(y, sy, ly)};
+  double r = 0, jx = 0, jy = 0;
+  for (int i = 0; i < 9; i++) {
+    const int slot = xs[sel(L::e(0, i))] + lx * ys[sel(L::e(1, i))];
+    const double v = weight<L>(i) + (double)load_dev(pop + i * pitch + slot, inv_scale);
+    if (f) f[(long long)i * lx * ly + k] = v;
+    r += v;
+    jx += L::e(0, i) * v;
+    jy += L::e(1, i) * v;
+  }
+  if (rho) rho[k] = r;
+  if (ux) ux[k] = jx / r;
+  if (uy) uy[k] = jy / r;
+}
+
+}  // namespace
+
+// Natural-layout fields of one domain: RHO, U_X, U_Y (N doubles; u = j/rho of
+// the current populations, without the Guo half-force shift) or F (9N).
+extern "C" lbmc_status lbmc_batch_fetch(lbmc_batch *b, int domain, int field, void *dst, size_t bytes) {
+  if (!b || !dst || domain < 0 || domain >= b->ndomains) return berr(LBMC_ERR_INVALID_ARG, "lbmc_batch_fetch");
+  const BatchDomainDev &D = b->dom[domain];
+  const long long n = (long long)D.lx * D.ly;
+  const size_t need = (size_t)n * 8 * (field == LBMC_FIELD_F ? 9 : 1);
+  if (field != LBMC_FIELD_RHO && field != LBMC_FIELD_U_X && field != LBMC_FIELD_U_Y && field != LBMC_FIELD_F)
+    return berr(LBMC_ERR_INVALID_ARG, "lbmc_batch_fetch: field");
+  if (bytes < need) return berr(LBMC_ERR_BUFFER_SIZE, "lbmc_batch_fetch: buffer too small");
+  cudaSetDevice(b->cfg.device);
+  BatchStateDev st;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(&st, b->state + domain, sizeof(st), cudaMemcpyDeviceToHost);
+  double *tmp = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, need);
+  if (e == cudaSuccess) {
+    double *rho = field == LBMC_FIELD_RHO ? tmp : nullptr;
+    double *ux = field == LBMC_FIELD_U_X ? tmp : nullptr;
+    double *uy = field == LBMC_FIELD_U_Y ? tmp : nullptr;
+    double *f = field == LBMC_FIELD_F ? tmp : nullptr;
+    const int nb = (int)((n + 255) / 256);
+    const float inv = (float)(1.0 / b->scale);
+    switch (b->cfg.storage) {
+      case LBMC_F16:
+        batch_fetch_kernel<__half><<<nb, 256, 0, b->stream>>>(
+            reinterpret_cast<const __half *>(b->pool) + D.pop_off, D.pitch, D.lx, D.ly, st.t, inv, rho, ux, uy, f);
+        break;
+      case LBMC_BF16:
+        batch_fetch_kernel<__nv_bfloat16><<<nb, 256, 0, b->stream>>>(
+            reinterpret_cast<const __nv_bfloat16 *>(b->pool) + D.pop_off, D.pitch, D.lx, D.ly, st.t, inv, rho,
+            ux, uy, f);
+        break;
+      default:
+        batch_fetch_kernel<float><<<nb, 256, 0, b->stream>>>(reinterpret_cast<const float *>(b->pool) + D.pop_off,
+                                                            D.pitch, D.lx, D.ly, st.t, inv, rho, ux, uy, f);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(dst, tmp, need, cudaMemcpyDeviceToHost);
+  }
+  if (tmp) cudaFree(tmp);
+  if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_fetch: ") + cudaGetErrorString(e));
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_batch_destroy(lbmc_batch *b) {
+  if (!b) return LBMC_OK;
+  cudaSetDevice(b->cfg.device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  void *ptrs[] = {b->pool, b->cls, b->B, b->u_prev, b->dom_dev, b->state, b->order_dev, b->counters, b->t0};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return LBMC_OK;
+}

@@ -98,6 +98,8 @@ struct HostClasses {
 
 }  // namespace
 
+void lbmc::set_last_error(const std::string &message) { g_last_error = message; }
+
 struct lbmc_handle {
   lbmc_config cfg;
   DeviceState ds;

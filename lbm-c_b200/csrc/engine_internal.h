@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 namespace lbmc {
 
 // Device-side state of one handle, in the form the launchers consume.
@@ -57,6 +59,9 @@ struct LatticeStorageOps {
   // Chooses the step kernel and launch geometry; sets nblocks.
   cudaError_t (*plan)(DeviceState &);
 };
+
+// Sets the calling thread's lbmc_last_error() message.
+void set_last_error(const std::string &message);
 
 const LatticeStorageOps *ops_d2q9_f32();
 const LatticeStorageOps *ops_d2q9_f16();

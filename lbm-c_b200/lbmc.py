@@ -273,3 +273,108 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+# ----------------------------------------------------------- batched domains
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("tau", ctypes.c_double), ("force", ctypes.c_double * 2),
+                ("collision_type", ctypes.c_int), ("storage", ctypes.c_int),
+                ("storage_scale", ctypes.c_double), ("device", ctypes.c_int),
+                ("block_threads", ctypes.c_int), ("steps_per_launch", ctypes.c_int),
+                ("reserved", ctypes.c_int * 8)]
+
+
+class BatchDomain(ctypes.Structure):
+    _fields_ = [("length", ctypes.c_int * 2), ("geometry", _DP)]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("delta_u", ctypes.c_double),
+                ("elapsed_ms", ctypes.c_double), ("converged", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
+
+
+def _batch_lib():
+    lib = library()
+    if not getattr(lib, "_batch_ready", False):
+        lib.lbmc_batch_init.argtypes = [ctypes.POINTER(BatchConfig), ctypes.c_int,
+                                        ctypes.POINTER(BatchDomain), ctypes.POINTER(_P)]
+        lib.lbmc_batch_run.argtypes = [_P, ctypes.c_longlong, ctypes.c_double, ctypes.c_int,
+                                       ctypes.POINTER(BatchResult)]
+        lib.lbmc_batch_fetch.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_size_t]
+        lib.lbmc_batch_info.argtypes = [_P, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]
+        lib.lbmc_batch_destroy.argtypes = [_P]
+        for name in ("lbmc_batch_init", "lbmc_batch_run", "lbmc_batch_fetch",
+                     "lbmc_batch_info", "lbmc_batch_destroy"):
+            getattr(lib, name).restype = ctypes.c_int
+        lib._batch_ready = True
+    return lib
+
+
+class Batch:
+    """Many independent D2Q9 domains in one persistent launch (lbmc_batch_*)."""
+
+    def __init__(self, geometries, tau=1.0, force=(1e-6, 0.0), collision_type=NTPOR,
+                 storage=F16, storage_scale=0.0, device=0, block_threads=0, steps_per_launch=0):
+        lib = _batch_lib()
+        cfg = BatchConfig()
+        cfg.tau = tau
+        cfg.force[0], cfg.force[1] = force
+        cfg.collision_type = collision_type
+        cfg.storage = STORAGE_IDS.get(storage, storage)
+        cfg.storage_scale = storage_scale
+        cfg.device = device
+        cfg.block_threads = block_threads
+        cfg.steps_per_launch = steps_per_launch
+        self._keep = []
+        doms = (BatchDomain * len(geometries))()
+        self.shapes = []
+        for d, g in enumerate(geometries):
+            g = np.ascontiguousarray(g, np.float64)
+            ly, lx = g.shape
+            doms[d].length[0], doms[d].length[1] = lx, ly
+            doms[d].geometry = g.ctypes.data_as(_DP)
+            self._keep.append(g)
+            self.shapes.append((ly, lx))
+        h = _P()
+        check(lib.lbmc_batch_init(ctypes.byref(cfg), len(geometries), doms, ctypes.byref(h)))
+        self.h, self.n = h, len(geometries)
+
+    def run(self, max_steps, tol, check_every=100):
+        res = (BatchResult * self.n)()
+        check(_batch_lib().lbmc_batch_run(self.h, max_steps, tol, check_every, res))
+        return res
+
+    def fetch(self, d, field):
+        ly, lx = self.shapes[d]
+        out = np.empty((9 if field == FIELD_F else 1) * lx * ly)
+        check(_batch_lib().lbmc_batch_fetch(self.h, d, field, out.ctypes.data_as(_P), out.nbytes))
+        return out.reshape(9, -1) if field == FIELD_F else out
+
+    def info(self):
+        tot, th, st, res = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(_batch_lib().lbmc_batch_info(self.h, ctypes.byref(tot), ctypes.byref(th),
+                                           ctypes.byref(st), ctypes.byref(res)))
+        return dict(total_nodes=tot.value, threads=th.value, steps_per_launch=st.value,
+                    resident_domains=res.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _batch_lib().lbmc_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

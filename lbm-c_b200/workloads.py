@@ -163,3 +163,43 @@ def engine_for(lbmc, w: Workload, storage="f32", **kw):
     eng = lbmc.Engine(cfg, dom)
     del keep
     return eng
+
+
+def imb_weight(eps, tau):
+    """Noble-Torczynski solid weight from area coverage:
+    B = eps (tau - 1/2) / ((1 - eps) + (tau - 1/2)); eps = 1 gives B = 1."""
+    return eps * (tau - 0.5) / ((1.0 - eps) + (tau - 0.5))
+
+
+def circle_domain(lx, ly, target, rng, rmin=3.0, rmax=12.0, tau=1.0):
+    """Porosity field (ly, lx) of random circles (radius U[rmin, rmax], uniform
+    periodic centres) added until the covered area reaches `target`.  Cell
+    coverage eps = clamp(r - |x_cell - c| + 1/2, 0, 1) (signed-distance area
+    estimate), union by maximum; B from imb_weight."""
+    eps = np.zeros((ly, lx))
+    while eps.mean() < target:
+        r = rng.uniform(rmin, rmax)
+        cx, cy = rng.uniform(0, lx), rng.uniform(0, ly)
+        R = int(np.ceil(r + 1))
+        xs = np.arange(int(np.floor(cx)) - R, int(np.floor(cx)) + R + 1)
+        ys = np.arange(int(np.floor(cy)) - R, int(np.floor(cy)) + R + 1)
+        dx = (xs + 0.5 - cx)[None, :]
+        dy = (ys + 0.5 - cy)[:, None]
+        cov = np.clip(r - np.sqrt(dx * dx + dy * dy) + 0.5, 0.0, 1.0)
+        ix, iy = np.mod(xs, lx), np.mod(ys, ly)
+        sub = eps[np.ix_(iy, ix)]
+        eps[np.ix_(iy, ix)] = np.maximum(sub, cov)
+    return imb_weight(eps, tau)
+
+
+def batch_sweep(n=4096, lmin=32, lmax=512, seed=5, tau=1.0, square=False):
+    """Config-5 style domains: sides log-uniform in [lmin, lmax] (independent
+    per axis unless square), solid fraction U[0.2, 0.5] of circles radius
+    3-12 with IMB edges."""
+    rng = np.random.default_rng(seed)
+    geoms = []
+    for _ in range(n):
+        lx = int(round(np.exp(rng.uniform(np.log(lmin), np.log(lmax)))))
+        ly = lx if square else int(round(np.exp(rng.uniform(np.log(lmin), np.log(lmax)))))
+        geoms.append(circle_domain(lx, ly, rng.uniform(0.2, 0.5), rng, tau=tau))
+    return geoms
