@@ -177,6 +177,7 @@ def dist_barrier(world: int, device=None):
 
 
 WORKLOAD_METRIC = {
+    "batch": "aggregate GLUPS ({n} D2Q9 domains, persistent batched launch, to steady state)",
     "porous": "GLUPS (D3Q15 MRT porous {n}^3 fused step)",
     "tgv": "GLUPS (D3Q15 BGK+Smagorinsky Taylor-Green {n}^3 fused step)",
     "poiseuille": "GLUPS (D2Q9 BGK+Guo Poiseuille 128x64 fused step)",
@@ -194,7 +195,103 @@ def build_workload(args):
 
 
 def metric_name(args):
+    if args.workload == "batch":
+        return WORKLOAD_METRIC["batch"].format(n=args.domains)
     return WORKLOAD_METRIC[args.workload].format(n=args.size)
+
+
+def run_batch(args, world, rank, local):
+    """Config-5 sweep: independent D2Q9 NTPOR+Guo domains (IMB circles), one
+    persistent launch replayed from a CUDA graph until every domain's
+    max |u(t) - u(t-1)| < tol.  Per-domain latency = device time from the
+    run's start to the domain's convergence; the comparison runs a seeded
+    sample of domains alone through lbmc_init/lbmc_iterate (one launch per
+    step), checking the same criterion every check_every steps."""
+    import torch
+
+    import lbmc
+    import workloads
+    torch.cuda.set_device(local)
+    tau, g, tol, check, cap = 1.0, 1e-6, 1e-9, 100, args.batch_cap
+    geoms = workloads.batch_sweep(args.domains, seed=5 + rank, tau=tau)
+    nodes = np.array([x.size for x in geoms])
+    # warm-up: a small batch (module load, autotuner paths)
+    with lbmc.Batch(geoms[:8], tau=tau, force=(g, 0.0), storage=args.storage) as wb:
+        wb.run(max(1, args.warmup) * check, 0.0, check)
+    dev = torch.device("cuda", local)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        b = lbmc.Batch(geoms, tau=tau, force=(g, 0.0), storage=args.storage)
+        t_init = time.perf_counter() - t0
+        t1 = time.perf_counter()
+        res = b.run(cap, tol, check)
+        torch.cuda.synchronize(dev)
+        t_run = time.perf_counter() - t1
+    info = b.info()
+    steps = np.array([r.steps for r in res])
+    conv = np.array([r.converged for r in res], bool)
+    lat = np.array([r.elapsed_ms for r in res])
+    b.close()
+    lups = float((steps * nodes).sum())
+    rate, t_max = aggregate_rate(lups, t_run, world, dev)
+    # alone: a sample of domains, each through the single-domain engine
+    rng = np.random.default_rng(11)
+    sample = rng.choice(len(geoms), size=min(args.alone_sample, len(geoms)), replace=False)
+    alone = []
+    for d in sample:
+        ly, lx = geoms[d].shape
+        n = lx * ly
+        force = np.zeros((2, n))
+        force[0] = g
+        cfg = lbmc.make_config("d2q9", (lx, ly, 1), tau=tau, collision_type=lbmc.NTPOR,
+                               forcing=True, storage=args.storage, device=local)
+        dom, keep = lbmc.make_domain(n, 2, 9, geoms[d].reshape(n), force)
+        torch.cuda.synchronize(dev)
+        ta = time.perf_counter()
+        with lbmc.Engine(cfg, dom) as e:
+            prev, done = None, 0
+            while done < cap:
+                e.iterate(check - 1, 0)
+                e.iterate(1, lbmc.STORE_MACROS)
+                done += check
+                u = e.u()
+                if prev is not None and np.abs(u - prev).max() < tol:
+                    break
+                prev = u
+        alone.append((time.perf_counter() - ta) * 1e3)
+        del keep
+    batched_sample = lat[sample]
+    if rank == 0:
+        line = {
+            "metric": metric_name(args), "value": rate / 1e9, "unit": UNIT, "n_gpus": world,
+            "steps": int(steps.max()), "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.storage, "data": "synthetic (seeded circles, IMB edges)",
+            "config": {"workload": "batch_d2q9_ntpor_guo_circles", "domains": args.domains,
+                       "total_nodes": int(nodes.sum()), "tau": tau, "g": g, "tol": tol,
+                       "check_every": check, "step_cap": cap,
+                       "sides": "log-uniform [32, 512] per axis",
+                       "threads": info["threads"], "steps_per_launch": info["steps_per_launch"],
+                       "resident_domains": info["resident_domains"],
+                       "parallelism": f"replicas{world}"},
+            "time_to_steady_s": float(np.nanmax(np.where(conv, lat, np.nan)) / 1e3) if conv.any() else None,
+            "run_s": t_run, "init_s": t_init,
+            "converged": int(conv.sum()), "unconverged": int((~conv).sum()),
+            "unconverged_delta_u_max": (float(max(r.delta_u for r, c in zip(res, conv) if not c))
+                                        if (~conv).any() else None),
+            "latency_ms": {"batched_p50": float(np.percentile(lat[conv], 50)) if conv.any() else None,
+                           "batched_p99": float(np.percentile(lat[conv], 99)) if conv.any() else None,
+                           "sample": len(sample),
+                           "sample_batched_p50": float(np.percentile(batched_sample, 50)),
+                           "sample_batched_p99": float(np.percentile(batched_sample, 99)),
+                           "sample_alone_p50": float(np.percentile(alone, 50)),
+                           "sample_alone_p99": float(np.percentile(alone, 99)),
+                           "alone_total_ms": float(np.sum(alone))},
+            "gpu_launches": None,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
 
 
 # --------------------------------------------------------------- CPU legs
@@ -404,6 +501,9 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--kernel", choices=["auto", "direct", "pipelined"], default="auto")
     ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
+    ap.add_argument("--domains", type=int, default=4096)
+    ap.add_argument("--batch-cap", type=int, default=200000)
+    ap.add_argument("--alone-sample", type=int, default=32)
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -416,6 +516,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, world, rank)
+        elif args.workload == "batch":
+            run_batch(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -11,7 +11,9 @@
 // K times in shared memory and written back, so its K steps cost one read and
 // one write of HBM; larger domains are stepped in HBM.  Every C steps a
 // domain compares u with the previous step (max norm) and freezes once below
-// the tolerance, recording the device timer.  The host replays a CUDA graph
+// the tolerance, recording the device timer.  Shared-memory-resident domains
+// and HBM domains run in two kernels launched as parallel branches of the
+// graph, each with its own queue and launch shape.  The host replays a CUDA graph
 // (queue reset + kernel) until all domains converged or hit the step cap.  An
 // autotuner times the first launches with several block sizes and K, keeps
 // the fastest.
@@ -54,10 +56,10 @@ struct BatchArgs {
   float2 *u_prev;
   const BatchDomainDev *dom;
   BatchStateDev *state;
-  const int *order;          // domains, largest first
-  int ndomains;
-  int *queue;                // atomic work counter (reset before each launch)
-  int *active;               // domains still running after this launch
+  const int *order;          // this kernel's domains, largest first
+  int ndomains;              // entries in order
+  int *queue;                // this kernel's atomic work counter (reset before each launch)
+  int *active;               // domains still running after this launch (both kernels)
   int steps;                 // K: steps per launch per domain
   int check;                 // C: convergence check interval
   float tol;
@@ -119,7 +121,10 @@ __device__ __forceinline__ float block_max(float v, float *sh) {
   return r;
 }
 
-template <class S, bool BLEND>
+// RESIDENT: the domains of this launch fit in shared memory (one block per
+// SM with the full shared-memory carve-out); otherwise they are stepped in
+// HBM by several smaller blocks per SM with no dynamic shared memory.
+template <class S, bool BLEND, bool RESIDENT>
 __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int sh_dom;
@@ -152,7 +157,7 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
     float2 *up = A.u_prev + D.node_off;
     S *pop = pool + D.pop_off;
     long long pitch = D.pitch;
-    if (D.resident) {
+    if (RESIDENT) {
       for (int i = 0; i < 9; i++)
         for (int k = threadIdx.x; k < n; k += blockDim.x) sbuf[(long long)i * n + k] = pop[(long long)i * D.pitch + k];
       pop = sbuf;
@@ -163,8 +168,11 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
     int stop = 0;
     for (int s = 0; s < A.steps && !stop; s++, t++) {
       const int sx = (int)(t % D.lx), sy = (int)(t % D.ly);
-      const bool save = ((t + 1) % A.check) == 0;
-      const bool test = t > 0 && (t % A.check) == 0;
+      // Every C steps: du = max |u(t) - u(t - C)|, then u(t) is kept for the
+      // next check.  Reduced-precision dynamics that settle into a fixed point
+      // or a cycle whose period divides C give exactly zero.
+      const bool save = (t % A.check) == 0;
+      const bool test = save && t >= A.check;
       float dmax = 0;
       for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int x = k % D.lx, y = k / D.lx;
@@ -189,7 +197,7 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
       }
       if (t + 1 >= A.max_steps) stop = stop ? stop : 2;
     }
-    if (D.resident) {
+    if (RESIDENT) {
       __syncthreads();
       for (int i = 0; i < 9; i++)
         for (int k = threadIdx.x; k < n; k += blockDim.x)
@@ -217,7 +225,8 @@ struct lbmc_batch {
   lbmc_batch_config cfg;
   int ndomains = 0;
   std::vector<BatchDomainDev> dom;
-  std::vector<int> order;
+  std::vector<int> order;      // resident domains, then HBM domains, each largest first
+  int n_resident = 0;
   void *pool = nullptr;
   uint8_t *cls = nullptr;
   float *B = nullptr;
@@ -225,7 +234,7 @@ struct lbmc_batch {
   BatchDomainDev *dom_dev = nullptr;
   BatchStateDev *state = nullptr;
   int *order_dev = nullptr;
-  int *counters = nullptr;  // [0] queue, [1] active
+  int *counters = nullptr;  // [0] resident queue, [1] HBM queue, [2] active
   unsigned long long *t0 = nullptr;
   cudaStream_t stream = nullptr;
   int ssize = 4;
@@ -234,6 +243,9 @@ struct lbmc_batch {
   size_t smem_bytes = 0;
   int sms = 0;
   int threads = 0, steps = 0;  // tuned launch shape
+  int hbm_blocks_per_sm[3] = {1, 1, 1};  // for 256 / 512 / 1024 threads
+  cudaStream_t side = nullptr;            // second graph branch
+  cudaEvent_t fork = nullptr, join = nullptr;
   double scale = 1;
 };
 
@@ -246,22 +258,44 @@ lbmc_status berr(lbmc_status s, const std::string &m) {
 
 template <class S>
 cudaError_t configure_batch(lbmc_batch *b) {
-  cudaError_t e = cudaFuncSetAttribute(batch_kernel<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)b->smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(batch_kernel<S, true, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem_bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(batch_kernel<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(batch_kernel<S, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)b->smem_bytes);
+  const int th[3] = {256, 512, 1024};
+  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &nb, b->blend ? batch_kernel<S, true, false> : batch_kernel<S, false, false>, th[k], 0);
+    b->hbm_blocks_per_sm[k] = nb > 0 ? nb : 1;
+  }
   return e;
 }
 
 template <class S>
-cudaError_t launch_batch(lbmc_batch *b, const BatchArgs &A, int threads, cudaStream_t st) {
-  auto kern = b->blend ? batch_kernel<S, true> : batch_kernel<S, false>;
-  kern<<<b->sms, threads, b->smem_bytes, st>>>(A);
-  return cudaGetLastError();
+cudaError_t launch_batch(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hbm, int threads,
+                         cudaStream_t st) {
+  // Resident domains on st, HBM domains on the side stream, joined again.
+  cudaError_t e = cudaEventRecord(b->fork, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->fork, 0);
+  if (e != cudaSuccess) return e;
+  if (res.ndomains > 0) {
+    auto kr = b->blend ? batch_kernel<S, true, true> : batch_kernel<S, false, true>;
+    kr<<<b->sms, threads, b->smem_bytes, st>>>(res);
+  }
+  if (hbm.ndomains > 0) {
+    const int k = threads <= 256 ? 0 : (threads <= 512 ? 1 : 2);
+    auto kh = b->blend ? batch_kernel<S, true, false> : batch_kernel<S, false, false>;
+    kh<<<b->sms * b->hbm_blocks_per_sm[k], threads, 0, b->side>>>(hbm);
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventRecord(b->join, b->side);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->join, 0);
+  return e;
 }
 
-BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long max_steps) {
+BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long max_steps, bool resident) {
   BatchArgs A;
   memset(&A, 0, sizeof(A));
   A.pool = b->pool;
@@ -270,10 +304,10 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
   A.u_prev = b->u_prev;
   A.dom = b->dom_dev;
   A.state = b->state;
-  A.order = b->order_dev;
-  A.ndomains = b->ndomains;
-  A.queue = b->counters;
-  A.active = b->counters + 1;
+  A.order = b->order_dev + (resident ? 0 : b->n_resident);
+  A.ndomains = resident ? b->n_resident : b->ndomains - b->n_resident;
+  A.queue = b->counters + (resident ? 0 : 1);
+  A.active = b->counters + 2;
   A.steps = steps;
   A.check = check;
   A.tol = (float)tol;
@@ -284,17 +318,20 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
   A.scale = (float)b->scale;
   A.inv_scale = (float)(1.0 / b->scale);
   A.blend = b->blend;
-  A.smem_elems = b->smem_bytes / b->ssize;
+  A.smem_elems = resident ? b->smem_bytes / b->ssize : 0;
   return A;
 }
 
-cudaError_t enqueue(lbmc_batch *b, const BatchArgs &A, int threads, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(b->counters, 0, 2 * sizeof(int), st);
+cudaError_t enqueue(lbmc_batch *b, int steps, int check, double tol, long long max_steps, int threads,
+                    cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, 3 * sizeof(int), st);
   if (e != cudaSuccess) return e;
+  const BatchArgs res = make_args(b, steps, check, tol, max_steps, true);
+  const BatchArgs hbm = make_args(b, steps, check, tol, max_steps, false);
   switch (b->cfg.storage) {
-    case LBMC_F16: return launch_batch<__half>(b, A, threads, st);
-    case LBMC_BF16: return launch_batch<__nv_bfloat16>(b, A, threads, st);
-    default: return launch_batch<float>(b, A, threads, st);
+    case LBMC_F16: return launch_batch<__half>(b, res, hbm, threads, st);
+    case LBMC_BF16: return launch_batch<__nv_bfloat16>(b, res, hbm, threads, st);
+    default: return launch_batch<float>(b, res, hbm, threads, st);
   }
 }
 
@@ -366,8 +403,10 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   b->order.resize(ndomains);
   std::iota(b->order.begin(), b->order.end(), 0);
   std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+    if (b->dom[x].resident != b->dom[y].resident) return b->dom[x].resident > b->dom[y].resident;
     return (long long)b->dom[x].lx * b->dom[x].ly > (long long)b->dom[y].lx * b->dom[y].ly;
   });
+  for (const auto &D : b->dom) b->n_resident += D.resident;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void **p, size_t bytes) {
     if (e == cudaSuccess) e = cudaMalloc(p, bytes ? bytes : 16);
@@ -379,7 +418,7 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   alloc((void **)&b->dom_dev, ndomains * sizeof(BatchDomainDev));
   alloc((void **)&b->state, ndomains * sizeof(BatchStateDev));
   alloc((void **)&b->order_dev, ndomains * sizeof(int));
-  alloc((void **)&b->counters, 2 * sizeof(int));
+  alloc((void **)&b->counters, 3 * sizeof(int));
   alloc((void **)&b->t0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(b->pool, 0, (size_t)pop * b->ssize);  // f = w (Init 0)
   if (e == cudaSuccess) e = cudaMemcpy(b->cls, cls.data(), node, cudaMemcpyHostToDevice);
@@ -391,6 +430,9 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   if (e == cudaSuccess)
     e = cudaMemcpy(b->order_dev, b->order.data(), ndomains * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
   if (e == cudaSuccess) {
     switch (cfg->storage) {
       case LBMC_F16: e = configure_batch<__half>(b); break;
@@ -430,9 +472,8 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
       for (int si = 0; si < 2; si++) {
         const int th = b->threads > 0 ? b->threads : cand_threads[ti];
         const int sp = b->steps > 0 ? b->steps : cand_steps[si];
-        const BatchArgs A = make_args(b, sp, check_every, tol, max_steps);
         cudaEventRecord(e0, b->stream);
-        e = enqueue(b, A, th, b->stream);
+        e = enqueue(b, sp, check_every, tol, max_steps, th, b->stream);
         cudaEventRecord(e1, b->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) break;
@@ -452,13 +493,12 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
     b->steps = bs;
   }
 
-  // Capture one launch (queue reset + kernel) in a graph and replay it.
-  const BatchArgs A = make_args(b, b->steps, check_every, tol, max_steps);
+  // Capture one launch (queue reset + both kernels) in a graph and replay it.
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    cudaError_t e2 = enqueue(b, A, b->threads, b->stream);
+    cudaError_t e2 = enqueue(b, b->steps, check_every, tol, max_steps, b->threads, b->stream);
     e = cudaStreamEndCapture(b->stream, &graph);
     if (e2 != cudaSuccess) e = e2;
   }
@@ -467,7 +507,7 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
   const long long launches_max = max_steps / std::max(1, b->steps) + 2;
   for (long long l = 0; e == cudaSuccess && active > 0 && l < launches_max; l++) {
     e = cudaGraphLaunch(exec, b->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&active, b->counters + 1, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&active, b->counters + 2, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   }
   if (exec) cudaGraphExecDestroy(exec);
@@ -585,6 +625,9 @@ extern "C" lbmc_status lbmc_batch_destroy(lbmc_batch *b) {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->side) cudaStreamDestroy(b->side);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->join) cudaEventDestroy(b->join);
   delete b;
   return LBMC_OK;
 }

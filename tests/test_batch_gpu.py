@@ -17,7 +17,7 @@ FORCE = (2e-5, -5e-6)
 def domains(seed=3):
     import workloads
     rng = np.random.default_rng(seed)
-    shapes = [(16, 24), (40, 33), (96, 120), (75, 160), (33, 64), (130, 90)]
+    shapes = [(16, 24), (40, 33), (96, 120), (75, 160), (33, 64), (130, 90), (90, 200)]
     return [workloads.circle_domain(lx, ly, rng.uniform(0.2, 0.4), rng, tau=TAU)
             for ly, lx in shapes]
 
