@@ -203,98 +203,116 @@ def metric_name(args):
 def run_batch(args, world, rank, local):
     """Config-5 sweep: independent D2Q9 NTPOR+Guo domains (IMB circles), one
     persistent launch replayed from a CUDA graph until every domain's
-    max |u(t) - u(t-1)| < tol.  Per-domain latency = device time from the
-    run's start to the domain's convergence; the comparison runs a seeded
-    sample of domains alone through lbmc_init/lbmc_iterate (one launch per
-    step), checking the same criterion every check_every steps."""
+    max |u(t) - u(t-C)| < tol (C = check interval).  Per-domain latency =
+    device time from the run's start to the domain's convergence; the
+    comparison runs a seeded sample of domains alone through
+    lbmc_init/lbmc_iterate (one launch per step) with the same criterion.
+
+    FP16 storage floors max|u(t) - u(t-C)| at ~1e-8..1e-6 (quantisation of
+    f - w), above the 1e-9 tolerance, in both paths; so the FP16 run is
+    bounded by --batch-cap and reports throughput and the floor, and the
+    time-to-steady / latency figures come from the FP32 run, which converges."""
     import torch
 
     import lbmc
     import workloads
     torch.cuda.set_device(local)
-    tau, g, tol, check, cap = 1.0, 1e-6, 1e-9, 100, args.batch_cap
+    dev = torch.device("cuda", local)
+    tau, g, tol, check = 1.0, 1e-6, 1e-9, 100
     geoms = workloads.batch_sweep(args.domains, seed=5 + rank, tau=tau)
     nodes = np.array([x.size for x in geoms])
-    # warm-up: a small batch (module load, autotuner paths)
     with lbmc.Batch(geoms[:8], tau=tau, force=(g, 0.0), storage=args.storage) as wb:
         wb.run(max(1, args.warmup) * check, 0.0, check)
-    dev = torch.device("cuda", local)
-    with ClockSampler(local) as clk:
+
+    def batched(storage, cap):
         torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        b = lbmc.Batch(geoms, tau=tau, force=(g, 0.0), storage=args.storage)
-        t_init = time.perf_counter() - t0
+        b = lbmc.Batch(geoms, tau=tau, force=(g, 0.0), storage=storage)
         t1 = time.perf_counter()
         res = b.run(cap, tol, check)
         torch.cuda.synchronize(dev)
         t_run = time.perf_counter() - t1
-    info = b.info()
-    steps = np.array([r.steps for r in res])
-    conv = np.array([r.converged for r in res], bool)
-    lat = np.array([r.elapsed_ms for r in res])
-    b.close()
-    lups = float((steps * nodes).sum())
-    rate, t_max = aggregate_rate(lups, t_run, world, dev)
-    # alone: a sample of domains, each through the single-domain engine
+        info = b.info()
+        b.close()
+        steps = np.array([r.steps for r in res])
+        conv = np.array([r.converged for r in res], bool)
+        lat = np.array([r.elapsed_ms for r in res])
+        du = np.array([r.delta_u for r in res])
+        rate, t_max = aggregate_rate(float((steps * nodes).sum()), t_run, world, dev)
+        out = {"storage": storage, "glups": rate / 1e9, "run_s": t_max, "step_cap": cap,
+               "max_steps": int(steps.max()), "converged": int(conv.sum()),
+               "unconverged": int((~conv).sum()), "threads": info["threads"],
+               "steps_per_launch": info["steps_per_launch"],
+               "resident_domains": info["resident_domains"]}
+        if conv.any():
+            out["time_to_steady_s"] = float(lat[conv].max() / 1e3)
+            out["latency_p50_ms"] = float(np.percentile(lat[conv], 50))
+            out["latency_p99_ms"] = float(np.percentile(lat[conv], 99))
+        if (~conv).any():
+            out["unconverged_delta_u"] = {"min": float(du[~conv].min()),
+                                          "median": float(np.median(du[~conv])),
+                                          "max": float(du[~conv].max())}
+        return out, lat, conv
+
+    with ClockSampler(local) as clk:
+        main, _, _ = batched(args.storage, args.batch_cap)
+    f32, lat32, conv32 = batched("f32", 400000) if args.storage != "f32" else (main, None, None)
+    if lat32 is None:
+        f32, lat32, conv32 = batched("f32", 400000)
+
+    # alone: a seeded sample of domains, each through the single-domain engine (FP32)
     rng = np.random.default_rng(11)
     sample = rng.choice(len(geoms), size=min(args.alone_sample, len(geoms)), replace=False)
-    alone = []
+    alone, alone_conv = [], []
     for d in sample:
         ly, lx = geoms[d].shape
         n = lx * ly
         force = np.zeros((2, n))
         force[0] = g
         cfg = lbmc.make_config("d2q9", (lx, ly, 1), tau=tau, collision_type=lbmc.NTPOR,
-                               forcing=True, storage=args.storage, device=local)
+                               forcing=True, storage="f32", device=local)
         dom, keep = lbmc.make_domain(n, 2, 9, geoms[d].reshape(n), force)
         torch.cuda.synchronize(dev)
         ta = time.perf_counter()
+        ok = False
         with lbmc.Engine(cfg, dom) as e:
             prev, done = None, 0
-            while done < cap:
+            while done < 400000:
                 e.iterate(check - 1, 0)
                 e.iterate(1, lbmc.STORE_MACROS)
                 done += check
                 u = e.u()
                 if prev is not None and np.abs(u - prev).max() < tol:
+                    ok = True
                     break
                 prev = u
         alone.append((time.perf_counter() - ta) * 1e3)
+        alone_conv.append(ok)
         del keep
-    batched_sample = lat[sample]
+    both = [i for i, d in enumerate(sample) if conv32[d] and alone_conv[i]]
     if rank == 0:
         line = {
-            "metric": metric_name(args), "value": rate / 1e9, "unit": UNIT, "n_gpus": world,
-            "steps": int(steps.max()), "warmup": args.warmup, "ms_per_step": None,
+            "metric": metric_name(args), "value": main["glups"], "unit": UNIT, "n_gpus": world,
+            "steps": main["max_steps"], "warmup": args.warmup, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.storage, "data": "synthetic (seeded circles, IMB edges)",
             "config": {"workload": "batch_d2q9_ntpor_guo_circles", "domains": args.domains,
                        "total_nodes": int(nodes.sum()), "tau": tau, "g": g, "tol": tol,
-                       "check_every": check, "step_cap": cap,
-                       "sides": "log-uniform [32, 512] per axis",
-                       "threads": info["threads"], "steps_per_launch": info["steps_per_launch"],
-                       "resident_domains": info["resident_domains"],
+                       "criterion": "max|u(t) - u(t-C)|, C = check_every",
+                       "check_every": check, "sides": "log-uniform [32, 512] per axis",
                        "parallelism": f"replicas{world}"},
-            "time_to_steady_s": float(np.nanmax(np.where(conv, lat, np.nan)) / 1e3) if conv.any() else None,
-            "run_s": t_run, "init_s": t_init,
-            "converged": int(conv.sum()), "unconverged": int((~conv).sum()),
-            "unconverged_delta_u_max": (float(max(r.delta_u for r, c in zip(res, conv) if not c))
-                                        if (~conv).any() else None),
-            "latency_ms": {"batched_p50": float(np.percentile(lat[conv], 50)) if conv.any() else None,
-                           "batched_p99": float(np.percentile(lat[conv], 99)) if conv.any() else None,
-                           "sample": len(sample),
-                           "sample_batched_p50": float(np.percentile(batched_sample, 50)),
-                           "sample_batched_p99": float(np.percentile(batched_sample, 99)),
-                           "sample_alone_p50": float(np.percentile(alone, 50)),
-                           "sample_alone_p99": float(np.percentile(alone, 99)),
-                           "alone_total_ms": float(np.sum(alone))},
+            "run": main, "fp32_run": f32,
+            "latency_vs_alone_fp32": {
+                "sample": len(sample), "both_converged": len(both),
+                "batched_p50_ms": float(np.percentile(lat32[sample[both]], 50)) if both else None,
+                "batched_p99_ms": float(np.percentile(lat32[sample[both]], 99)) if both else None,
+                "alone_p50_ms": float(np.percentile(np.array(alone)[both], 50)) if both else None,
+                "alone_p99_ms": float(np.percentile(np.array(alone)[both], 99)) if both else None,
+                "alone_sequential_total_ms": float(np.sum(alone))},
             "gpu_launches": None,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
 
-
-# --------------------------------------------------------------- CPU legs
 
 class ReferenceTimer:
     """The host-compiled reference step on a crop (z, or y for 2-D) of the
@@ -502,7 +520,7 @@ def main():
     ap.add_argument("--kernel", choices=["auto", "direct", "pipelined"], default="auto")
     ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
     ap.add_argument("--domains", type=int, default=4096)
-    ap.add_argument("--batch-cap", type=int, default=200000)
+    ap.add_argument("--batch-cap", type=int, default=20000)
     ap.add_argument("--alone-sample", type=int, default=32)
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
