@@ -278,6 +278,42 @@ lbmc_status lbmc_batch_info(lbmc_batch *b, long long *total_nodes, int *threads,
                             int *steps_per_launch, int *resident_domains);
 lbmc_status lbmc_batch_destroy(lbmc_batch *b);
 
+/* ---------------- learned subgrid closure (no reference counterpart) ------
+ * A 6 -> 32 -> 32 -> 1 SiLU MLP (1313 parameters, BF16 weights, FP32
+ * accumulation) maps six invariants of the local strain-rate estimate to an
+ * eddy viscosity nu_t; tau_eff = tau + 3 nu_t.  Trained on the GPU by the
+ * library's own forward/backward/Adam kernels.  Attached to a BGK-family
+ * handle it replaces Smagorinsky (LBM-C/collision.cu:445-463), which stays
+ * the fallback wherever the inputs leave the training range. */
+typedef struct lbmc_mlp lbmc_mlp;
+
+lbmc_status lbmc_mlp_create(int device, unsigned long long seed, lbmc_mlp **out);
+/* Input normalisation x = (f - mean)/std, the normalised training range
+ * [lo, hi] per input (NULL = unbounded) and the target scale
+ * (nu_t = target_scale * output). */
+lbmc_status lbmc_mlp_set_normalization(lbmc_mlp *m, const float *mean, const float *std,
+                                       const float *lo, const float *hi, float target_scale);
+/* Six features per sample from strain tensors S (xx, yy, zz, xy, yz, xz) and
+ * densities (NULL = 1), computed by the same device function the step uses. */
+lbmc_status lbmc_mlp_features(int device, const float *strain6, const float *rho, long long n,
+                              float *features6);
+/* Mini-batch Adam on the mean squared error between target_scale * output
+ * and target; features are raw (normalised inside).  loss_history: epochs
+ * floats or NULL. */
+lbmc_status lbmc_mlp_train(lbmc_mlp *m, const float *features, const float *target, long long n,
+                           int epochs, int batch, float lr, float *loss_history);
+/* Gradient (1313 floats, parameter layout W1[32x6], b1, W2[32x32], b2, W3,
+ * b3) and value of the loss over one batch of n samples. */
+lbmc_status lbmc_mlp_gradients(lbmc_mlp *m, const float *features, const float *target, long long n,
+                               float *grads, float *loss);
+lbmc_status lbmc_mlp_predict(lbmc_mlp *m, const float *features, long long n, float *out);
+lbmc_status lbmc_mlp_get_params(lbmc_mlp *m, float *params);
+lbmc_status lbmc_mlp_set_params(lbmc_mlp *m, const float *params);
+lbmc_status lbmc_mlp_destroy(lbmc_mlp *m);
+/* Attaches (m != NULL) or detaches (m == NULL) the learned closure on a
+ * BGK-family handle; iterations = fixed-point passes for tau_eff (1..8). */
+lbmc_status lbmc_set_closure(lbmc_handle *h, const lbmc_mlp *m, int iterations);
+
 /* Host-only helpers (no GPU needed). */
 
 /* Checks a configuration and domain the way lbmc_init does, without touching

@@ -25,6 +25,7 @@
 #include "engine_internal.h"
 #include "kernels.cuh"
 #include "lattice.cuh"
+#include "mlp.cuh"
 
 using namespace lbmc;
 
@@ -648,6 +649,31 @@ extern "C" lbmc_status lbmc_destroy(lbmc_handle *h) {
   cudaSetDevice(h->cfg.device);
   cudaStreamSynchronize(h->stream);
   release(h);
+  return LBMC_OK;
+}
+
+// Defined in mlp.cu: the host copy of a network's closure parameters.
+const MlpClosure *lbmc_mlp_closure(const lbmc_mlp *m);
+
+extern "C" lbmc_status lbmc_set_closure(lbmc_handle *h, const lbmc_mlp *m, int iterations) {
+  if (!h) return fail(LBMC_ERR_INVALID_ARG, "lbmc_set_closure: handle is NULL");
+  if (h->cfg.collision_type != LBMC_BGK && h->cfg.collision_type != LBMC_NTPOR)
+    return fail(LBMC_ERR_UNSUPPORTED, "the learned closure replaces Smagorinsky: BGK family only");
+  CK(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(h->stream), "lbmc_set_closure");
+  if (!m) {  // detach: back to Smagorinsky / plain BGK
+    h->ds.col = h->cfg.c_smag > 0 ? COL_BGK_SMAG : COL_BGK;
+    return LBMC_OK;
+  }
+  if (iterations < 1 || iterations > 8) return fail(LBMC_ERR_INVALID_ARG, "iterations must be 1..8");
+  MlpClosure c = *lbmc_mlp_closure(m);
+  c.iterations = iterations;
+  if (!h->ds.closure) {
+    lbmc_status s = dev_alloc(h, &h->ds.closure, sizeof(MlpClosure), "closure");
+    if (s != LBMC_OK) return s;
+  }
+  CK(cudaMemcpy(h->ds.closure, &c, sizeof(c), cudaMemcpyHostToDevice), "upload closure");
+  h->ds.col = COL_BGK_MLP;
   return LBMC_OK;
 }
 

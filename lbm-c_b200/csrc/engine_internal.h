@@ -43,6 +43,7 @@ struct DeviceState {
   int stages;               // shared-memory stages of the pipelined kernel
   long long pipe_grid;      // persistent blocks of the pipelined kernel
   long long nblocks;        // blocks of the step kernel (diagnostic partials)
+  void *closure;            // device MlpClosure when a learned closure is attached
 };
 
 struct LatticeStorageOps {
@@ -62,6 +63,8 @@ struct LatticeStorageOps {
 
 // Sets the calling thread's lbmc_last_error() message.
 void set_last_error(const std::string &message);
+
+struct MlpClosure;
 
 const LatticeStorageOps *ops_d2q9_f32();
 const LatticeStorageOps *ops_d2q9_f16();

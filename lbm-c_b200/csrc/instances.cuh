@@ -43,6 +43,7 @@ struct Launchers {
     a.rows = (long long)d.L[1] * d.L[2];
     a.stages = d.stages;
     a.table = d.table_dev;
+    a.closure = static_cast<const MlpClosure *>(d.closure);
     return a;
   }
 
@@ -124,6 +125,7 @@ struct Launchers {
       case COL_BGK: e = launch_col<COL_BGK>(a, d, diag, st); break;
       case COL_BGK_SMAG: e = launch_col<COL_BGK_SMAG>(a, d, diag, st); break;
       case COL_MRT_NC: e = launch_col<COL_MRT_NC>(a, d, diag, st); break;
+      case COL_BGK_MLP: e = launch_col<COL_BGK_MLP>(a, d, diag, st); break;
       default: e = launch_col<COL_MRT>(a, d, diag, st); break;
     }
     if (e != cudaSuccess) return e;
@@ -154,6 +156,7 @@ struct Launchers {
       case COL_BGK: probe(step_pipelined_kernel<L, S, COL_BGK, true, true, true>); break;
       case COL_BGK_SMAG: probe(step_pipelined_kernel<L, S, COL_BGK_SMAG, true, true, true>); break;
       case COL_MRT_NC: probe(step_pipelined_kernel<L, S, COL_MRT_NC, true, true, true>); break;
+      case COL_BGK_MLP: probe(step_pipelined_kernel<L, S, COL_BGK_MLP, true, true, true>); break;
       default: probe(step_pipelined_kernel<L, S, COL_MRT, true, true, true>); break;
     }
     if (e != cudaSuccess) return e;

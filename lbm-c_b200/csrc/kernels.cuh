@@ -25,6 +25,7 @@
 #include <utility>
 
 #include "lattice.cuh"
+#include "mlp.cuh"
 
 namespace lbmc {
 
@@ -129,6 +130,7 @@ constexpr int COL_BGK = 0;
 constexpr int COL_BGK_SMAG = 1;
 constexpr int COL_MRT = 2;
 constexpr int COL_MRT_NC = 3;  // MRT whose rates on rho and j are zero
+constexpr int COL_BGK_MLP = 4; // BGK family with the learned closure (Smagorinsky fallback)
 
 // rho and the momentum components (the conserved moments).
 template <class L>
@@ -173,6 +175,7 @@ struct StepArgs {
   long long rows;               // Ly * Lz (pipelined kernel)
   int stages;                   // shared-memory stages (pipelined kernel)
   const uint16_t *table;        // 256 class-table entries (device memory)
+  const MlpClosure *closure;    // learned closure (COL_BGK_MLP)
 };
 
 constexpr unsigned ERROR_TIMEOUT = 1u;
@@ -750,7 +753,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
     const C usq = C(1.5) * (nd.u[0] * nd.u[0] + nd.u[1] * nd.u[1] + nd.u[2] * nd.u[2]);
     const C A0 = C(weight<L>(0)) * (nd.drho - nd.rho * usq);
     C tau = tau0;
-    if constexpr (COL == COL_BGK_SMAG) {
+    if constexpr (COL == COL_BGK_SMAG || COL == COL_BGK_MLP) {
       // Smagorinsky (collision.cu:445-463, q_bar zeroed): q_ab = sum e_a e_b
       // (f - f_eq) is even in e, so each pair contributes e_a e_b (S - 2A).
       C q[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, yz, xz
@@ -771,7 +774,34 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       C qhat = r2 * (fabs(q[0]) + fabs(q[1]) + C(2) * fabs(q[3]));
       if (L::DIM > 2) qhat += r2 * (fabs(q[2]) + C(2) * (fabs(q[4]) + fabs(q[5])));
       const C k = C(2) * r2 * a.c_smag * a.c_smag * (C(9) / nd.rho);
-      tau = tau0 + C(0.5) * (sqrt(tau0 * tau0 + k * qhat) - tau0);
+      const C tau_smag = tau0 + C(0.5) * (sqrt(tau0 * tau0 + k * qhat) - tau0);
+      if constexpr (COL == COL_BGK_SMAG) {
+        tau = tau_smag;
+      } else {
+        // Learned closure: strain estimate S = -3 q / (2 rho tau) from the
+        // non-equilibrium stress (c_s^2 = 1/3), six invariants, MLP -> nu_t,
+        // tau = tau0 + 3 nu_t, repeated `iterations` times so that S uses the
+        // effective tau.  Outside the normalised training range: Smagorinsky.
+        const MlpClosure *cl = a.closure;
+        bool in_range = true;
+        for (int it = 0; it < cl->iterations && in_range; it++) {
+          const float ks = -1.5f / ((float)nd.rho * (float)tau);
+          float Sm[6], f[MLP_IN];
+#pragma unroll
+          for (int c = 0; c < 6; c++) Sm[c] = ks * (float)q[c];
+          strain_features(Sm, (float)nd.rho, f);
+#pragma unroll
+          for (int c = 0; c < MLP_IN; c++) {
+            f[c] = (f[c] - cl->mean[c]) * cl->inv_std[c];
+            in_range = in_range && f[c] >= cl->lo[c] && f[c] <= cl->hi[c];
+          }
+          if (in_range) {
+            const float nu = fmaxf(0.0f, cl->target_scale * mlp_forward(cl->w, f));
+            tau = tau0 + C(3) * C(nu);
+          }
+        }
+        if (!in_range) tau = tau_smag;
+      }
     }
     const C om = C(1) / tau;
     // population 0 (e = 0)
@@ -871,9 +901,9 @@ __device__ __forceinline__ void block_diag(const double (&v)[DIAG_VALUES], bool 
 // Grid: blockDim (bx, 1, 1) along x, gridDim (ceil(Lx/bx), Ly, Lz).
 template <class S, int COL>
 constexpr int direct_min_blocks() {
-  // FP64 arithmetic needs register pairs: no cap beyond the 128 per thread
-  // that 8 resident blocks imply.
-  if (std::is_same<S, double>::value) return 8;
+  // FP64 arithmetic needs register pairs, the learned closure its hidden
+  // layer: no cap beyond the 128 per thread that 8 resident blocks imply.
+  if (std::is_same<S, double>::value || COL == COL_BGK_MLP) return 8;
   return COL == COL_BGK_SMAG ? DIRECT_MIN_BLOCKS_SMAG : DIRECT_MIN_BLOCKS;
 }
 

@@ -378,3 +378,110 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------ learned closure
+
+MLP_PARAMS = 1313
+
+
+def _mlp_lib():
+    lib = library()
+    if not getattr(lib, "_mlp_ready", False):
+        lib.lbmc_mlp_create.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(_P)]
+        lib.lbmc_mlp_set_normalization.argtypes = [_P, _P, _P, _P, _P, ctypes.c_float]
+        lib.lbmc_mlp_features.argtypes = [ctypes.c_int, _P, _P, ctypes.c_longlong, _P]
+        lib.lbmc_mlp_train.argtypes = [_P, _P, _P, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_float, _P]
+        lib.lbmc_mlp_gradients.argtypes = [_P, _P, _P, ctypes.c_longlong, _P,
+                                           ctypes.POINTER(ctypes.c_float)]
+        lib.lbmc_mlp_predict.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.lbmc_mlp_get_params.argtypes = [_P, _P]
+        lib.lbmc_mlp_set_params.argtypes = [_P, _P]
+        lib.lbmc_mlp_destroy.argtypes = [_P]
+        lib.lbmc_set_closure.argtypes = [_P, _P, ctypes.c_int]
+        for name in ("lbmc_mlp_create", "lbmc_mlp_set_normalization", "lbmc_mlp_features",
+                     "lbmc_mlp_train", "lbmc_mlp_gradients", "lbmc_mlp_predict",
+                     "lbmc_mlp_get_params", "lbmc_mlp_set_params", "lbmc_mlp_destroy",
+                     "lbmc_set_closure"):
+            getattr(lib, name).restype = ctypes.c_int
+        lib._mlp_ready = True
+    return lib
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, np.float32)
+    return a if shape is None else a.reshape(shape)
+
+
+def mlp_features(strain6, rho=None, device=0):
+    """Six closure inputs per sample from strain tensors (n, 6) and densities."""
+    S = _f32(strain6, (-1, 6))
+    n = S.shape[0]
+    r = None if rho is None else _f32(rho, (n,))
+    out = np.empty((n, 6), np.float32)
+    check(_mlp_lib().lbmc_mlp_features(device, S.ctypes.data, None if r is None else r.ctypes.data,
+                                       n, out.ctypes.data))
+    return out
+
+
+class Mlp:
+    """The closure network (lbmc_mlp_*)."""
+
+    def __init__(self, seed=0, device=0):
+        h = _P()
+        check(_mlp_lib().lbmc_mlp_create(device, seed, ctypes.byref(h)))
+        self.h = h
+
+    def set_normalization(self, mean, std, lo=None, hi=None, target_scale=1.0):
+        m, s = _f32(mean), _f32(std)
+        lo = None if lo is None else _f32(lo)
+        hi = None if hi is None else _f32(hi)
+        self._norm = (m, s, lo, hi)
+        check(_mlp_lib().lbmc_mlp_set_normalization(
+            self.h, m.ctypes.data, s.ctypes.data, None if lo is None else lo.ctypes.data,
+            None if hi is None else hi.ctypes.data, target_scale))
+
+    def train(self, features, target, epochs=10, batch=4096, lr=1e-3):
+        X, y = _f32(features, (-1, 6)), _f32(target, (-1,))
+        hist = np.zeros(epochs, np.float32)
+        check(_mlp_lib().lbmc_mlp_train(self.h, X.ctypes.data, y.ctypes.data, X.shape[0], epochs,
+                                        batch, lr, hist.ctypes.data))
+        return hist
+
+    def gradients(self, features, target):
+        X, y = _f32(features, (-1, 6)), _f32(target, (-1,))
+        g = np.empty(MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        check(_mlp_lib().lbmc_mlp_gradients(self.h, X.ctypes.data, y.ctypes.data, X.shape[0],
+                                            g.ctypes.data, ctypes.byref(loss)))
+        return g, loss.value
+
+    def predict(self, features):
+        X = _f32(features, (-1, 6))
+        out = np.empty(X.shape[0], np.float32)
+        check(_mlp_lib().lbmc_mlp_predict(self.h, X.ctypes.data, X.shape[0], out.ctypes.data))
+        return out
+
+    def params(self):
+        p = np.empty(MLP_PARAMS, np.float32)
+        check(_mlp_lib().lbmc_mlp_get_params(self.h, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = _f32(p)
+        check(_mlp_lib().lbmc_mlp_set_params(self.h, p.ctypes.data))
+
+    def attach(self, engine, iterations=2):
+        check(_mlp_lib().lbmc_set_closure(engine.h, self.h, iterations))
+
+    def close(self):
+        if getattr(self, "h", None):
+            _mlp_lib().lbmc_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

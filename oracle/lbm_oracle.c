@@ -62,6 +62,7 @@ typedef struct {
   double *f, *g; /* current / next, Q*N natural layout */
   double *geometry, *force, *u, *rho;
   int *macro, *micro;
+  const double *tau_field; /* per-node relaxation time replacing Smagorinsky, or NULL */
   long step;
 } orc_state;
 
@@ -311,7 +312,10 @@ static void collide(const orc_state *s, node_t *nd, double tau, int solid) {
       guo_force_terms(s, nd, tau, ft);
     }
     equilibrium(s, nd, feq);
-    if (nd->c_smag > 0) turbulent_viscosity(s, nd, feq, &tau);
+    /* A closure supplies the node's relaxation time where the reference
+       would call turbulent_viscosity; the Guo terms keep tau0, as there. */
+    if (s->tau_field) tau = s->tau_field[nd->ixd];
+    else if (nd->c_smag > 0) turbulent_viscosity(s, nd, feq, &tau);
     if (type == 0) {
       for (int i = 0; i < q; i++) {
         if (forcing)
@@ -617,6 +621,10 @@ void orc_equilibrium_field(const orc_state *s, const double *rho, const double *
     for (int i = 0; i < s->q; i++) out[i * n + k] = feq[i];
   }
 }
+
+/* Per-node relaxation times for the next steps (NULL restores tau/Smagorinsky);
+   the caller keeps the array alive. */
+void orc_set_tau_field(orc_state *s, const double *tau) { s->tau_field = tau; }
 
 void orc_destroy(orc_state *s) {
   if (!s) return;

@@ -121,6 +121,7 @@ class Restatement:
         lib.orc_destroy.argtypes = [_P]
         lib.orc_tables.argtypes = [_P] * 6
         lib.orc_equilibrium_field.argtypes = [_P] * 4
+        lib.orc_set_tau_field.argtypes = [_P, _P]
         self.lib, self.case = lib, case
         cfg = _OrcConfig()
         cfg.lattice = LATTICES[case.lattice][0]
@@ -168,6 +169,11 @@ class Restatement:
         u = np.ascontiguousarray(u, np.float64)
         self.lib.orc_equilibrium_field(self.h, _ptr(rho), _ptr(u), _ptr(out))
         return out
+
+    def set_tau_field(self, tau):
+        """Per-node relaxation times (N) for the following steps, or None."""
+        self._tau = None if tau is None else np.ascontiguousarray(tau, np.float64)
+        self.lib.orc_set_tau_field(self.h, _ptr(self._tau))
 
     def close(self):
         if self.h:
