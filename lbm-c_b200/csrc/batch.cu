@@ -429,6 +429,9 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   if (e == cudaSuccess) e = cudaMemset(b->state, 0, ndomains * sizeof(BatchStateDev));
   if (e == cudaSuccess)
     e = cudaMemcpy(b->order_dev, b->order.data(), ndomains * sizeof(int), cudaMemcpyHostToDevice);
+  // A host-to-device cudaMemcpy from pageable memory may return before its
+  // DMA lands, and the non-blocking streams below do not wait for it.
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);

@@ -504,7 +504,9 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
           host[k] = rho * w * (1.0 + eu + 0.5 * eu * eu - 1.5 * usq);
         }
       }
-      cudaError_t e = cudaMemcpy(tmp, host.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+      // Ordered on the handle's stream: a pageable cudaMemcpy may return
+      // before its DMA lands, and the non-blocking stream would not wait.
+      cudaError_t e = cudaMemcpyAsync(tmp, host.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
       if (e == cudaSuccess) e = h->ops->upload_population(d, 0, i, tmp, h->stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
       if (e != cudaSuccess) s2 = cuda_fail(e, "upload initial populations");
@@ -672,7 +674,8 @@ extern "C" lbmc_status lbmc_set_closure(lbmc_handle *h, const lbmc_mlp *m, int i
     lbmc_status s = dev_alloc(h, &h->ds.closure, sizeof(MlpClosure), "closure");
     if (s != LBMC_OK) return s;
   }
-  CK(cudaMemcpy(h->ds.closure, &c, sizeof(c), cudaMemcpyHostToDevice), "upload closure");
+  CK(cudaMemcpyAsync(h->ds.closure, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream), "upload closure");
+  CK(cudaStreamSynchronize(h->stream), "upload closure");
   h->ds.col = COL_BGK_MLP;
   return LBMC_OK;
 }

@@ -226,6 +226,29 @@ def test_init_equilibrium(lbmc):
         np.testing.assert_allclose(eng.f(), expect, rtol=0, atol=1e-15)
 
 
+@pytest.mark.parametrize("length,init", [((64, 64, 64), "eq"), ((96, 96, 96), "eq"), ((64, 64, 64), "f")])
+def test_init_large_is_exact_and_repeatable(lbmc, length, init):
+    """Large initial states arrive whole: every population of every node
+    equals f_eq(rho, u) (or the given f), on two builds in a row.  The
+    staging copy of each population is ordered on the handle's stream; a
+    pageable cudaMemcpy followed by a kernel on a non-blocking stream let
+    the kernel read the previous population's tail."""
+    n = int(np.prod(length))
+    rng = np.random.default_rng(3)
+    rho = 1 + 0.01 * rng.standard_normal(n)
+    u = 0.03 * rng.standard_normal((3, n))
+    case = make_case("d3q15", length, seed=1)
+    case.rho, case.u, case.f0 = rho, u, None
+    expect = Restatement(case).equilibrium(rho, u)
+    if init == "f":
+        case.f0 = expect + 1e-3 * rng.standard_normal(expect.shape)
+        expect = case.f0
+    kind = lbmc.INIT_EQUILIBRIUM if init == "eq" else lbmc.INIT_F
+    for _ in range(2):
+        with lbmc.Engine.from_case(case, init_type=kind, storage=lbmc.F64) as eng:
+            np.testing.assert_allclose(eng.f(), expect, rtol=0, atol=1e-15)
+
+
 @pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
 def test_pipelined_and_direct_kernels_agree(lbmc, storage):
     """The two step kernels compute the same thing: identical bits."""
