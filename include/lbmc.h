@@ -307,6 +307,9 @@ lbmc_status lbmc_mlp_train(lbmc_mlp *m, const float *features, const float *targ
 lbmc_status lbmc_mlp_gradients(lbmc_mlp *m, const float *features, const float *target, long long n,
                                float *grads, float *loss);
 lbmc_status lbmc_mlp_predict(lbmc_mlp *m, const float *features, long long n, float *out);
+/* The same prediction as the step computes it: warp-wide on the tensor
+ * cores, BF16 inputs and activations, FP32 accumulation, BF16 SiLU. */
+lbmc_status lbmc_mlp_predict_step(lbmc_mlp *m, const float *features, long long n, float *out);
 lbmc_status lbmc_mlp_get_params(lbmc_mlp *m, float *params);
 lbmc_status lbmc_mlp_set_params(lbmc_mlp *m, const float *params);
 lbmc_status lbmc_mlp_destroy(lbmc_mlp *m);

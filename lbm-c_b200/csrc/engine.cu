@@ -668,10 +668,14 @@ extern "C" lbmc_status lbmc_set_closure(lbmc_handle *h, const lbmc_mlp *m, int i
     return LBMC_OK;
   }
   if (iterations < 1 || iterations > 8) return fail(LBMC_ERR_INVALID_ARG, "iterations must be 1..8");
-  MlpClosure c = *lbmc_mlp_closure(m);
-  c.iterations = iterations;
+  if (h->ds.use_pipeline)
+    return fail(LBMC_ERR_UNSUPPORTED, "the learned closure runs in the direct-load kernel (lbmc_config.kernel)");
+  // The step evaluates the network warp-wide on the tensor cores, from the
+  // weights in fragment order; the scalars travel with each launch.
+  MlpStep c;
+  mlp_step_layout(*lbmc_mlp_closure(m), iterations, c, h->ds.closure_consts);
   if (!h->ds.closure) {
-    lbmc_status s = dev_alloc(h, &h->ds.closure, sizeof(MlpClosure), "closure");
+    lbmc_status s = dev_alloc(h, &h->ds.closure, sizeof(MlpStep), "closure");
     if (s != LBMC_OK) return s;
   }
   CK(cudaMemcpyAsync(h->ds.closure, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream), "upload closure");

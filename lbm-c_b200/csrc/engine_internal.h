@@ -7,6 +7,8 @@
 
 #include <string>
 
+#include "mlp.cuh"
+
 namespace lbmc {
 
 // Device-side state of one handle, in the form the launchers consume.
@@ -43,7 +45,8 @@ struct DeviceState {
   int stages;               // shared-memory stages of the pipelined kernel
   long long pipe_grid;      // persistent blocks of the pipelined kernel
   long long nblocks;        // blocks of the step kernel (diagnostic partials)
-  void *closure;            // device MlpClosure when a learned closure is attached
+  void *closure;            // device MlpStep when a learned closure is attached
+  lbmc::MlpConsts closure_consts;  // its scalars, passed with each launch
 };
 
 struct LatticeStorageOps {

@@ -43,7 +43,8 @@ struct Launchers {
     a.rows = (long long)d.L[1] * d.L[2];
     a.stages = d.stages;
     a.table = d.table_dev;
-    a.closure = static_cast<const MlpClosure *>(d.closure);
+    a.closure = static_cast<const MlpStep *>(d.closure);
+    a.mlp = d.closure_consts;
     return a;
   }
 
@@ -80,19 +81,23 @@ struct Launchers {
 
   template <int COL, bool FORCE, bool BLEND, bool DIAG>
   static cudaError_t launch(const StepArgs<C> &a, const DeviceState &d, cudaStream_t st) {
-    if (d.use_pipeline) {
-      auto kern = step_pipelined_kernel<L, S, COL, FORCE, BLEND, DIAG>;
-      const size_t smem = (size_t)d.stages * stage_bytes(d);
-      static thread_local size_t configured = 0;  // per instantiation
-      if (configured < smem) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = smem;
+    // The learned closure evaluates its network warp-wide, which the direct
+    // kernel's converged warps allow: it never runs in the pipelined kernel.
+    if constexpr (COL != COL_BGK_MLP) {
+      if (d.use_pipeline) {
+        auto kern = step_pipelined_kernel<L, S, COL, FORCE, BLEND, DIAG>;
+        const size_t smem = (size_t)d.stages * stage_bytes(d);
+        static thread_local size_t configured = 0;  // per instantiation
+        if (configured < smem) {
+          cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+          if (e != cudaSuccess) return e;
+          configured = smem;
+        }
+        kern<<<(unsigned)d.pipe_grid, pipe_threads(d), smem, st>>>(a);
+        return cudaSuccess;
       }
-      kern<<<(unsigned)d.pipe_grid, pipe_threads(d), smem, st>>>(a);
-    } else {
-      step_kernel<L, S, COL, FORCE, BLEND, DIAG><<<grid_dim(d), block_dim(d), 0, st>>>(a);
     }
+    step_kernel<L, S, COL, FORCE, BLEND, DIAG><<<grid_dim(d), block_dim(d), 0, st>>>(a);
     return cudaSuccess;
   }
 
@@ -156,7 +161,6 @@ struct Launchers {
       case COL_BGK: probe(step_pipelined_kernel<L, S, COL_BGK, true, true, true>); break;
       case COL_BGK_SMAG: probe(step_pipelined_kernel<L, S, COL_BGK_SMAG, true, true, true>); break;
       case COL_MRT_NC: probe(step_pipelined_kernel<L, S, COL_MRT_NC, true, true, true>); break;
-      case COL_BGK_MLP: probe(step_pipelined_kernel<L, S, COL_BGK_MLP, true, true, true>); break;
       default: probe(step_pipelined_kernel<L, S, COL_MRT, true, true, true>); break;
     }
     if (e != cudaSuccess) return e;

@@ -175,7 +175,8 @@ struct StepArgs {
   long long rows;               // Ly * Lz (pipelined kernel)
   int stages;                   // shared-memory stages (pipelined kernel)
   const uint16_t *table;        // 256 class-table entries (device memory)
-  const MlpClosure *closure;    // learned closure (COL_BGK_MLP)
+  const MlpStep *closure;       // learned closure (COL_BGK_MLP): weights
+  MlpConsts mlp;                // and its scalars
 };
 
 constexpr unsigned ERROR_TIMEOUT = 1u;
@@ -588,9 +589,11 @@ __device__ __forceinline__ void mrt_d3q15(const Node<D3Q15, C> &nd, const C *sra
 // (i, o = opp(i)), e_o = -e_i and w_o = w_i, so the equilibria, Guo terms
 // and the MRT transforms split into even and odd parts computed once per
 // pair.  Post-collision deviations go to out[].
+// `participate` (learned closure only): false for the lanes that only
+// accompany the warp-wide network evaluation (solid or out-of-range nodes).
 template <class L, class C, int COL, bool FORCE, bool BLEND>
 __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> &a, int n,
-                                              unsigned entry, C (&out)[L::Q]) {
+                                              unsigned entry, C (&out)[L::Q], bool participate = true) {
   constexpr int Q = L::Q;
   C B = 0;
   if (entry) {
@@ -779,28 +782,33 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
         tau = tau_smag;
       } else {
         // Learned closure: strain estimate S = -3 q / (2 rho tau) from the
-        // non-equilibrium stress (c_s^2 = 1/3), six invariants, MLP -> nu_t,
-        // tau = tau0 + 3 nu_t, repeated `iterations` times so that S uses the
-        // effective tau.  Outside the normalised training range: Smagorinsky.
-        const MlpClosure *cl = a.closure;
-        bool in_range = true;
-        for (int it = 0; it < cl->iterations && in_range; it++) {
-          const float ks = -1.5f / ((float)nd.rho * (float)tau);
+        // non-equilibrium stress (c_s^2 = 1/3), six invariants, network ->
+        // nu_t, tau = tau0 + 3 nu_t; the fixed point starts from the
+        // Smagorinsky tau and takes `iterations` passes.  Outside the
+        // normalised training range: Smagorinsky.  The network runs
+        // warp-wide on the tensor cores, so every lane of the warp takes the
+        // same number of passes (non-participating lanes feed zeros).
+        __shared__ __align__(16) unsigned mlp_stage[DIRECT_BLOCK / 32][128];
+        const MlpStep *cl = a.closure;
+        bool in_range = participate;
+        C tau_l = tau_smag;
+        for (int it = 0; it < a.mlp.iterations; it++) {
+          const float ks = __fdividef(-1.5f, (float)(nd.rho * tau_l));
           float Sm[6], f[MLP_IN];
 #pragma unroll
           for (int c = 0; c < 6; c++) Sm[c] = ks * (float)q[c];
           strain_features(Sm, (float)nd.rho, f);
 #pragma unroll
           for (int c = 0; c < MLP_IN; c++) {
-            f[c] = (f[c] - cl->mean[c]) * cl->inv_std[c];
-            in_range = in_range && f[c] >= cl->lo[c] && f[c] <= cl->hi[c];
+            f[c] = fmaf(f[c], a.mlp.scale[c], a.mlp.shift[c]);
+            in_range = in_range && f[c] >= a.mlp.lo[c] && f[c] <= a.mlp.hi[c];
           }
-          if (in_range) {
-            const float nu = fmaxf(0.0f, cl->target_scale * mlp_forward(cl->w, f));
-            tau = tau0 + C(3) * C(nu);
-          }
+#pragma unroll
+          for (int c = 0; c < MLP_IN; c++) f[c] = in_range ? f[c] : 0.0f;
+          const float y = mlp_forward_warp(cl, f, mlp_stage[threadIdx.x >> 5]) + a.mlp.b3;
+          if (in_range) tau_l = tau0 + C(3) * C(fmaxf(0.0f, a.mlp.target_scale * y));
         }
-        if (!in_range) tau = tau_smag;
+        tau = in_range ? tau_l : tau_smag;
       }
     }
     const C om = C(1) / tau;
@@ -914,33 +922,56 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
   constexpr int Q = L::Q;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = x < a.L[0];
-  if (!DIAG && !active) return;
+  // The learned closure's network runs warp-wide: every lane of a warp with
+  // an active node takes the node path, the others as non-participants.
+  constexpr bool WARP_WIDE = COL == COL_BGK_MLP;
+  const bool run = WARP_WIDE ? __any_sync(0xffffffffu, active) : active;
+  if (!DIAG && !run) return;
   double dv[DIAG_VALUES] = {0, 0, 0, 0, 0};
   bool nonfinite = false;
-  if (active) {
+  if (run) {
     const C inv_scale = a.inv_scale, scale = a.scale;
     Sites st;
-    st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
-    const int n = x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z);
+    const int n = active ? x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z) : 0;
     S *f = reinterpret_cast<S *>(a.f);
     Node<L, C> nd;
-    unroll<Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      nd.g[i] = load_dev(f + i * a.pitch + st.template slot<L>(i), inv_scale);
-    });
-    const int cls = a.cls[n];
+    if (active) {
+      st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
+      unroll<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        nd.g[i] = load_dev(f + i * a.pitch + st.template slot<L>(i), inv_scale);
+      });
+    } else {
+      unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = C(0); });
+    }
+    const int cls = active ? a.cls[n] : CLASS_SOLID;
     C out[Q];
-    if (cls == CLASS_SOLID) {
+    if constexpr (WARP_WIDE) {
+      // Solid and inactive lanes run the fluid update at rest (rho = 1,
+      // u = 0, no boundary entry) for the warp's sake, then bounce back.
+      const bool fluid = cls != CLASS_SOLID;
+      if (fluid) {
+        moments(nd);
+      } else {
+        nd.drho = 0;
+        nd.rho = 1;
+        nd.u[0] = nd.u[1] = nd.u[2] = 0;
+      }
+      collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, fluid && cls ? a.table[cls] : 0u, out, fluid);
+      if (!fluid) collide_solid(nd, out);
+    } else if (cls == CLASS_SOLID) {
       collide_solid(nd, out);
     } else {
       moments(nd);
       collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
     }
-    unroll<Q>([&](auto ic) {
-      constexpr int i = decltype(ic)::value;
-      store_dev(f + i * a.pitch + st.template slot<L>(i), out[i], scale);
-    });
-    store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
+    if (active) {
+      unroll<Q>([&](auto ic) {
+        constexpr int i = decltype(ic)::value;
+        store_dev(f + i * a.pitch + st.template slot<L>(i), out[i], scale);
+      });
+      store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
+    }
   }
   if (DIAG)
     block_diag<C>(dv, nonfinite, a,

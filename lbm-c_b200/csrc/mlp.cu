@@ -140,6 +140,19 @@ __global__ void mlp_predict_kernel(const float *xn, long long n, const __nv_bflo
   out[k] = scale * mlp_forward(w, x);
 }
 
+// The in-step evaluation (mlp_forward_warp) over a batch: 32 samples per
+// warp, lanes past n feed zeros.
+constexpr int STEP_PREDICT_BLOCK = 128;
+__global__ void __launch_bounds__(STEP_PREDICT_BLOCK)
+    mlp_predict_step_kernel(const float *raw, long long n, const MlpStep *cl, const MlpConsts kc, float *out) {
+  __shared__ __align__(16) unsigned stage[STEP_PREDICT_BLOCK / 32][128];
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float x[MLP_IN];
+  for (int i = 0; i < MLP_IN; i++) x[i] = k < n ? fmaf(raw[k * MLP_IN + i], kc.scale[i], kc.shift[i]) : 0.0f;
+  const float y = mlp_forward_warp(cl, x, stage[threadIdx.x >> 5]) + kc.b3;
+  if (k < n) out[k] = kc.target_scale * y;
+}
+
 __global__ void features_kernel(const float *S, const float *rho, long long n, float *out) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -174,6 +187,57 @@ void sync_host_weights(lbmc_mlp *m) {
 }  // namespace
 
 const MlpClosure *lbmc_mlp_closure(const lbmc_mlp *m) { return m ? &m->host : nullptr; }
+
+namespace lbmc {
+
+void mlp_step_layout(const MlpClosure &cl, int iterations, MlpStep &s, MlpConsts &kc) {
+  memset(&s, 0, sizeof(s));
+  memset(&kc, 0, sizeof(kc));
+  // BF16 bit pattern of parameter p, times `scale` (1 or the exact 1/2 that
+  // the in-step SiLU expects folded into layers 1 and 2).
+  auto bits = [&](int p, float scale) -> unsigned {
+    if (p < 0) return 0u;
+    const __nv_bfloat16 v = __float2bfloat16_rn(scale * __bfloat162float(cl.w[p]));
+    unsigned short b;
+    memcpy(&b, &v, sizeof(b));
+    return b;
+  };
+  auto pair = [&](int p0, int p1, float scale) -> unsigned {
+    return bits(p0, scale) | (bits(p1, scale) << 16);
+  };
+  auto set = [](uint4 &v, int j, unsigned w) { (j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w) = w; };
+  for (int lane = 0; lane < 32; lane++) {
+    const int g = lane >> 2, c = lane & 3;
+    for (int j = 0; j < 4; j++) {
+      const int n = 8 * j + g, k = 2 * c, col = 8 * j + 2 * c;
+      set(s.w1[lane], j, pair(k < MLP_IN ? MLP_W1 + n * MLP_IN + k : -1,
+                              k + 1 < MLP_IN ? MLP_W1 + n * MLP_IN + k + 1 : -1, 0.5f));
+      for (int kt = 0; kt < 2; kt++)
+        for (int r = 0; r < 2; r++) {
+          const int kk = 16 * kt + 8 * r + 2 * c;
+          set(s.w2[j][lane], 2 * kt + r, pair(MLP_W2 + n * MLP_H + kk, MLP_W2 + n * MLP_H + kk + 1, 0.5f));
+        }
+      set(s.b1[lane], j, pair(MLP_B1 + col, MLP_B1 + col + 1, 0.5f));
+      set(s.b2[lane], j, pair(MLP_B2 + col, MLP_B2 + col + 1, 0.5f));
+    }
+    for (int kt = 0; kt < 2; kt++)
+      for (int r = 0; r < 2; r++) {
+        const int kk = 16 * kt + 8 * r + 2 * c;
+        set(s.w3[lane], 2 * kt + r, g == 0 ? pair(MLP_W3 + kk, MLP_W3 + kk + 1, 1.0f) : 0u);
+      }
+  }
+  for (int i = 0; i < MLP_IN; i++) {
+    kc.scale[i] = cl.inv_std[i];
+    kc.shift[i] = -cl.mean[i] * cl.inv_std[i];
+    kc.lo[i] = cl.lo[i];
+    kc.hi[i] = cl.hi[i];
+  }
+  kc.b3 = __bfloat162float(cl.w[MLP_B3]);
+  kc.target_scale = cl.target_scale;
+  kc.iterations = iterations;
+}
+
+}  // namespace lbmc
 
 extern "C" lbmc_status lbmc_mlp_create(int device, unsigned long long seed, lbmc_mlp **out) {
   if (!out) return merr(LBMC_ERR_INVALID_ARG, "lbmc_mlp_create: out is NULL");
@@ -344,6 +408,30 @@ extern "C" lbmc_status lbmc_mlp_predict(lbmc_mlp *m, const float *features, long
   cudaFree(xn);
   cudaFree(res);
   if (e != cudaSuccess) return merr(LBMC_ERR_CUDA, std::string("lbmc_mlp_predict: ") + cudaGetErrorString(e));
+  return LBMC_OK;
+}
+
+extern "C" lbmc_status lbmc_mlp_predict_step(lbmc_mlp *m, const float *features, long long n, float *out) {
+  if (!m || !features || !out || n < 1) return merr(LBMC_ERR_INVALID_ARG, "lbmc_mlp_predict_step");
+  cudaSetDevice(m->device);
+  MlpStep hs;
+  MlpConsts kc;
+  mlp_step_layout(m->host, 1, hs, kc);
+  float *raw = nullptr, *res = nullptr;
+  MlpStep *ds = nullptr;
+  cudaError_t e = upload(&raw, features, (size_t)n * MLP_IN);
+  if (e == cudaSuccess) e = upload(&ds, &hs, 1);
+  if (e == cudaSuccess) e = cudaMalloc(&res, (size_t)n * sizeof(float));
+  if (e == cudaSuccess) {
+    const long long blocks = (n + STEP_PREDICT_BLOCK - 1) / STEP_PREDICT_BLOCK;
+    mlp_predict_step_kernel<<<(unsigned)blocks, STEP_PREDICT_BLOCK>>>(raw, n, ds, kc, res);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, res, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(raw);
+  cudaFree(ds);
+  cudaFree(res);
+  if (e != cudaSuccess) return merr(LBMC_ERR_CUDA, std::string("lbmc_mlp_predict_step: ") + cudaGetErrorString(e));
   return LBMC_OK;
 }
 

@@ -396,12 +396,13 @@ def _mlp_lib():
         lib.lbmc_mlp_gradients.argtypes = [_P, _P, _P, ctypes.c_longlong, _P,
                                            ctypes.POINTER(ctypes.c_float)]
         lib.lbmc_mlp_predict.argtypes = [_P, _P, ctypes.c_longlong, _P]
+        lib.lbmc_mlp_predict_step.argtypes = [_P, _P, ctypes.c_longlong, _P]
         lib.lbmc_mlp_get_params.argtypes = [_P, _P]
         lib.lbmc_mlp_set_params.argtypes = [_P, _P]
         lib.lbmc_mlp_destroy.argtypes = [_P]
         lib.lbmc_set_closure.argtypes = [_P, _P, ctypes.c_int]
         for name in ("lbmc_mlp_create", "lbmc_mlp_set_normalization", "lbmc_mlp_features",
-                     "lbmc_mlp_train", "lbmc_mlp_gradients", "lbmc_mlp_predict",
+                     "lbmc_mlp_train", "lbmc_mlp_gradients", "lbmc_mlp_predict", "lbmc_mlp_predict_step",
                      "lbmc_mlp_get_params", "lbmc_mlp_set_params", "lbmc_mlp_destroy",
                      "lbmc_set_closure"):
             getattr(lib, name).restype = ctypes.c_int
@@ -461,6 +462,13 @@ class Mlp:
         X = _f32(features, (-1, 6))
         out = np.empty(X.shape[0], np.float32)
         check(_mlp_lib().lbmc_mlp_predict(self.h, X.ctypes.data, X.shape[0], out.ctypes.data))
+        return out
+
+    def predict_step(self, features):
+        """The prediction as the step computes it (tensor cores, BF16 activations)."""
+        X = _f32(features, (-1, 6))
+        out = np.empty(X.shape[0], np.float32)
+        check(_mlp_lib().lbmc_mlp_predict_step(self.h, X.ctypes.data, X.shape[0], out.ctypes.data))
         return out
 
     def params(self):
