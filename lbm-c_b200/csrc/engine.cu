@@ -166,8 +166,8 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     return fail(LBMC_ERR_INVALID_ARG, "unknown storage %d", cfg->storage);
   if (cfg->streaming != LBMC_STREAM_SHIFT && cfg->streaming != LBMC_STREAM_AA)
     return fail(LBMC_ERR_INVALID_ARG, "unknown streaming scheme %d", cfg->streaming);
-  if (cfg->streaming == LBMC_STREAM_AA)
-    return fail(LBMC_ERR_UNSUPPORTED, "AA-pattern streaming is not available in this build");
+  if (cfg->streaming == LBMC_STREAM_AA && cfg->kernel == LBMC_KERNEL_PIPELINED)
+    return fail(LBMC_ERR_UNSUPPORTED, "AA-pattern streaming runs in the direct-load kernel only");
   if (cfg->init_type < 0 || cfg->init_type > 2)
     return fail(LBMC_ERR_INVALID_ARG, "unknown init type %d", cfg->init_type);
   if (cfg->compat & ~(LBMC_COMPAT_REFERENCE_AS_IS))
@@ -464,6 +464,7 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     // Every device-side wait gives up after about two seconds.
     d.timeout_cycles = (long long)(khz > 0 ? khz : 2000000) * 1000LL * 2;
   }
+  d.aa = cfg->streaming == LBMC_STREAM_AA ? 1 : 0;
   d.pipeline = cfg->kernel == LBMC_KERNEL_PIPELINED ? 2 : 0;
   TRYCUDA(h->ops->plan(d), "kernel planning");
   if (cfg->kernel == LBMC_KERNEL_PIPELINED && !d.use_pipeline) {

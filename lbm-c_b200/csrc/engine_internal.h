@@ -40,6 +40,7 @@ struct DeviceState {
   uint16_t *table_dev;      // device copy of table
   unsigned *error_flag;     // device word, ERROR_TIMEOUT on an expired wait
   long long timeout_cycles; // bound of every device-side wait
+  int aa;                   // AA-pattern layout (else the shift layout)
   int pipeline;             // allow the bulk-copy pipelined kernel
   int use_pipeline;         // chosen by plan()
   int stages;               // shared-memory stages of the pipelined kernel

@@ -22,8 +22,10 @@ struct Launchers {
       a.force_u[k] = (C)d.force_u[k];
       a.u[k] = static_cast<C *>(d.u[k]);
       a.L[k] = d.L[k];
-      a.s[k] = (int)(t % d.L[k]);
+      a.s[k] = d.aa ? (int)((t & 1) % d.L[k]) : (int)(t % d.L[k]);
     }
+    a.aa = d.aa;
+    a.odd = (int)(t & 1);
     a.rho = static_cast<C *>(d.rho);
     a.sf_buf = static_cast<const C *>(d.sf_buf);
     a.sf_index = d.sf_index;
@@ -97,7 +99,12 @@ struct Launchers {
         return cudaSuccess;
       }
     }
-    step_kernel<L, S, COL, FORCE, BLEND, DIAG><<<grid_dim(d), block_dim(d), 0, st>>>(a);
+    if (!d.aa)
+      step_kernel<L, S, COL, FORCE, BLEND, DIAG, STREAM_SHIFT><<<grid_dim(d), block_dim(d), 0, st>>>(a);
+    else if (a.odd)
+      step_kernel<L, S, COL, FORCE, BLEND, DIAG, STREAM_AA_ODD><<<grid_dim(d), block_dim(d), 0, st>>>(a);
+    else
+      step_kernel<L, S, COL, FORCE, BLEND, DIAG, STREAM_AA_EVEN><<<grid_dim(d), block_dim(d), 0, st>>>(a);
     return cudaSuccess;
   }
 
@@ -142,7 +149,7 @@ struct Launchers {
   static cudaError_t plan(DeviceState &d) {
     // The direct-load kernel is the default; the bulk-copy pipeline runs when
     // asked for (lbmc_config.kernel) and the rows allow it.
-    d.use_pipeline = (d.pipeline == 2 && pipelined_eligible(d)) ? 1 : 0;
+    d.use_pipeline = (d.pipeline == 2 && !d.aa && pipelined_eligible(d)) ? 1 : 0;
     if (!d.use_pipeline) {
       d.nblocks = blocks(d);
       return cudaSuccess;

@@ -162,7 +162,9 @@ struct StepArgs {
   double *diag_partials;  // DIAG_VALUES per block
   unsigned *diag_flag;    // bit 0: a non-finite rho/u was seen
   int L[3];
-  int s[3];  // shift of the current step: t mod L
+  int s[3];  // shift of the current step: t mod L (AA: t mod 2, wrapped by L)
+  int aa;    // AA-pattern layout (lbmc_streaming)
+  int odd;   // AA: the current step is odd
   int n;
   C tau;
   C s_mrt[15];
@@ -224,6 +226,27 @@ struct Sites {
     return x[sel(L::e(0, i))] + row[sel(L::e(1, i))][sel(L::e(2, i))];
   }
 };
+
+// Streaming layouts of the direct step kernel.  SHIFT: population i of node
+// x at step t sits in slot (i, (x - t e_i) mod L) and the result goes back
+// to the same slot.  AA pattern (one array, natural node order, two index
+// maps): at an even step population i of node x is read from (i, x) and
+// the post-collision value of population i goes to (opp(i), x); at an odd
+// step population i is read from (opp(i), x - e_i) and written to
+// (i, x + e_i).  In both AA maps out[i] goes to the slot population opp(i)
+// was read from, so a node writes exactly the slots it read (in place, no
+// race), and the AA-odd read map is the shift map at t = 1 with the arrays
+// swapped pairwise.  The state after every step is the same as SHIFT's;
+// only where each value sits differs.
+constexpr int STREAM_SHIFT = 0, STREAM_AA_EVEN = 1, STREAM_AA_ODD = 2;
+
+// Array index and slot of population i of a node for the cold kernels
+// (stress-free gather, fetch, upload), from the runtime layout flags.
+template <class L, int I, class C>
+__device__ __forceinline__ long long natural_slot(const StepArgs<C> &a, const Sites &st) {
+  const int arr = (a.aa && a.odd) ? L::opp(I) : I;
+  return (long long)arr * a.pitch + st.template slot<L>(I);
+}
 
 // -------------------------------------------------------------- physics
 
@@ -915,7 +938,7 @@ constexpr int direct_min_blocks() {
   return COL == COL_BGK_SMAG ? DIRECT_MIN_BLOCKS_SMAG : DIRECT_MIN_BLOCKS;
 }
 
-template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG>
+template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG, int STREAM>
 __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
     step_kernel(const StepArgs<typename Storage<S>::C> a) {
   using C = typename Storage<S>::C;
@@ -935,12 +958,23 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
     const int n = active ? x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z) : 0;
     S *f = reinterpret_cast<S *>(a.f);
     Node<L, C> nd;
+    // Read slot of population i: (i, slot(i)) in the shift layout, (i, n)
+    // at an AA-even step, (opp(i), slot(i)) with the t = 1 shift at an
+    // AA-odd step; out[i] goes back to slot(i) (shift) or to population
+    // opp(i)'s read slot (AA).
+    auto read_at = [&](auto ic) -> S * {
+      constexpr int i = decltype(ic)::value;
+      if constexpr (STREAM == STREAM_AA_EVEN) return f + i * a.pitch + n;
+      else if constexpr (STREAM == STREAM_AA_ODD) return f + L::opp(i) * a.pitch + st.template slot<L>(i);
+      else return f + i * a.pitch + st.template slot<L>(i);
+    };
+    auto write_at = [&](auto ic) -> S * {
+      if constexpr (STREAM == STREAM_SHIFT) return read_at(ic);
+      else return read_at(std::integral_constant<int, L::opp(decltype(ic)::value)>{});
+    };
     if (active) {
-      st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
-      unroll<Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        nd.g[i] = load_dev(f + i * a.pitch + st.template slot<L>(i), inv_scale);
-      });
+      if constexpr (STREAM != STREAM_AA_EVEN) st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
+      unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(ic), inv_scale); });
     } else {
       unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = C(0); });
     }
@@ -966,10 +1000,7 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
       collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
     }
     if (active) {
-      unroll<Q>([&](auto ic) {
-        constexpr int i = decltype(ic)::value;
-        store_dev(f + i * a.pitch + st.template slot<L>(i), out[i], scale);
-      });
+      unroll<Q>([&](auto ic) { store_dev(write_at(ic), out[decltype(ic)::value], scale); });
       store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
     }
   }
@@ -1258,8 +1289,7 @@ __global__ void sf_gather_kernel(const StepArgs<typename Storage<S>::C> a,
       if constexpr (sf_unknown<L>(decltype(fc)::value, i)) need |= (face == decltype(fc)::value);
     });
     if (need)
-      sf_buf[(long long)k * L::Q + i] =
-          load_dev(f + i * a.pitch + st.template slot<L>(i), a.inv_scale);
+      sf_buf[(long long)k * L::Q + i] = load_dev(f + natural_slot<L, i>(a, st), a.inv_scale);
   });
 }
 
@@ -1276,8 +1306,7 @@ __global__ void fetch_population_kernel(const StepArgs<typename Storage<S>::C> a
   const S *f = reinterpret_cast<const S *>(a.f);
   unroll<L::Q>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
-    if (k == i)
-      out[n] = weight<L>(k) + (double)load_dev(f + k * a.pitch + st.template slot<L>(k), a.inv_scale);
+    if (k == i) out[n] = weight<L>(k) + (double)load_dev(f + natural_slot<L, k>(a, st), a.inv_scale);
   });
 }
 
@@ -1295,8 +1324,7 @@ __global__ void upload_population_kernel(const StepArgs<typename Storage<S>::C> 
   S *f = reinterpret_cast<S *>(a.f);
   unroll<L::Q>([&](auto kc) {
     constexpr int k = decltype(kc)::value;
-    if (k == i)
-      store_dev(f + k * a.pitch + st.template slot<L>(k), (C)(in[n] - weight<L>(k)), a.scale);
+    if (k == i) store_dev(f + natural_slot<L, k>(a, st), (C)(in[n] - weight<L>(k)), a.scale);
   });
 }
 
