@@ -416,7 +416,8 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.Stream(device)
     kernel = {"auto": lbmc.KERNEL_AUTO, "direct": lbmc.KERNEL_DIRECT,
               "pipelined": lbmc.KERNEL_PIPELINED}[args.kernel]
-    eng = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel)
+    streaming = lbmc.STREAM_AA if args.streaming == "aa" else lbmc.STREAM_SHIFT
+    eng = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel, streaming=streaming)
     lbmc.check(lbmc.library().lbmc_set_stream(eng.h, stream.cuda_stream))
     # warm-up
     eng.iterate(args.warmup, lbmc.SYNC)
@@ -458,7 +459,8 @@ def run_ours(args, world, rank, local):
         for k in range(args.e2e_reps + 1):
             torch.cuda.synchronize(device)
             t = time.perf_counter()
-            e = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel)
+            e = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel,
+                                     streaming=streaming)
             e.iterate(E2E_STEPS, lbmc.STORE_MACROS | lbmc.SYNC)
             e.rho()
             e.u()
@@ -485,7 +487,7 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.storage, "data": "synthetic (seeded)",
             "config": {"workload": w.name, "length": list(w.length), "nodes": w.n,
-                       "storage": args.storage,
+                       "storage": args.storage, "streaming": args.streaming,
                        "compute": "f32" if args.storage != "f64" else "f64",
                        "params": {k: (round(v, 6) if isinstance(v, float) else v)
                                   for k, v in w.params.items()},
@@ -518,6 +520,7 @@ def main():
     ap.add_argument("--storage", choices=list(STORAGE_BYTES), default="f32")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--kernel", choices=["auto", "direct", "pipelined"], default="auto")
+    ap.add_argument("--streaming", choices=["shift", "aa"], default="shift")
     ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
     ap.add_argument("--domains", type=int, default=4096)
     ap.add_argument("--batch-cap", type=int, default=20000)

@@ -945,45 +945,65 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
   constexpr int Q = L::Q;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = x < a.L[0];
-  // The learned closure's network runs warp-wide: every lane of a warp with
-  // an active node takes the node path, the others as non-participants.
-  constexpr bool WARP_WIDE = COL == COL_BGK_MLP;
-  const bool run = WARP_WIDE ? __any_sync(0xffffffffu, active) : active;
-  if (!DIAG && !run) return;
+  // Read slot of population i: (i, slot(i)) in the shift layout, (i, n) at
+  // an AA-even step, (opp(i), slot(i)) with the t = 1 shift at an AA-odd
+  // step; out[i] goes back to slot(i) (shift) or to population opp(i)'s
+  // read slot (AA).
+  auto read_at = [&](S *f, const Sites &st, int n, auto ic) -> S * {
+    constexpr int i = decltype(ic)::value;
+    if constexpr (STREAM == STREAM_AA_EVEN) return f + i * a.pitch + n;
+    else if constexpr (STREAM == STREAM_AA_ODD) return f + L::opp(i) * a.pitch + st.template slot<L>(i);
+    else return f + i * a.pitch + st.template slot<L>(i);
+  };
+  auto write_at = [&](S *f, const Sites &st, int n, auto ic) -> S * {
+    if constexpr (STREAM == STREAM_SHIFT) return read_at(f, st, n, ic);
+    else return read_at(f, st, n, std::integral_constant<int, L::opp(decltype(ic)::value)>{});
+  };
   double dv[DIAG_VALUES] = {0, 0, 0, 0, 0};
   bool nonfinite = false;
-  if (run) {
-    const C inv_scale = a.inv_scale, scale = a.scale;
-    Sites st;
-    const int n = active ? x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z) : 0;
-    S *f = reinterpret_cast<S *>(a.f);
-    Node<L, C> nd;
-    // Read slot of population i: (i, slot(i)) in the shift layout, (i, n)
-    // at an AA-even step, (opp(i), slot(i)) with the t = 1 shift at an
-    // AA-odd step; out[i] goes back to slot(i) (shift) or to population
-    // opp(i)'s read slot (AA).
-    auto read_at = [&](auto ic) -> S * {
-      constexpr int i = decltype(ic)::value;
-      if constexpr (STREAM == STREAM_AA_EVEN) return f + i * a.pitch + n;
-      else if constexpr (STREAM == STREAM_AA_ODD) return f + L::opp(i) * a.pitch + st.template slot<L>(i);
-      else return f + i * a.pitch + st.template slot<L>(i);
-    };
-    auto write_at = [&](auto ic) -> S * {
-      if constexpr (STREAM == STREAM_SHIFT) return read_at(ic);
-      else return read_at(std::integral_constant<int, L::opp(decltype(ic)::value)>{});
-    };
+  if constexpr (COL != COL_BGK_MLP) {
+    if (!DIAG && !active) return;
     if (active) {
+      const C inv_scale = a.inv_scale, scale = a.scale;
+      Sites st;
       if constexpr (STREAM != STREAM_AA_EVEN) st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
-      unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(ic), inv_scale); });
-    } else {
-      unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = C(0); });
+      const int n = x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z);
+      S *f = reinterpret_cast<S *>(a.f);
+      Node<L, C> nd;
+      unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(f, st, n, ic), inv_scale); });
+      const int cls = a.cls[n];
+      C out[Q];
+      if (cls == CLASS_SOLID) {
+        collide_solid(nd, out);
+      } else {
+        moments(nd);
+        collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
+      }
+      unroll<Q>([&](auto ic) { store_dev(write_at(f, st, n, ic), out[decltype(ic)::value], scale); });
+      store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
     }
-    const int cls = active ? a.cls[n] : CLASS_SOLID;
-    C out[Q];
-    if constexpr (WARP_WIDE) {
-      // Solid and inactive lanes run the fluid update at rest (rho = 1,
-      // u = 0, no boundary entry) for the warp's sake, then bounce back.
+  } else {
+    // The learned closure's network runs warp-wide: every lane of a warp
+    // with an active node takes the node path, the others (solid or past the
+    // edge) as non-participants that run the fluid update at rest (rho = 1,
+    // u = 0, no boundary entry) and then bounce back.
+    const bool run = __any_sync(0xffffffffu, active);
+    if (!DIAG && !run) return;
+    if (run) {
+      const C inv_scale = a.inv_scale, scale = a.scale;
+      Sites st;
+      const int n = active ? x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z) : 0;
+      S *f = reinterpret_cast<S *>(a.f);
+      Node<L, C> nd;
+      if (active) {
+        if constexpr (STREAM != STREAM_AA_EVEN) st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
+        unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(f, st, n, ic), inv_scale); });
+      } else {
+        unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = C(0); });
+      }
+      const int cls = active ? a.cls[n] : CLASS_SOLID;
       const bool fluid = cls != CLASS_SOLID;
+      C out[Q];
       if (fluid) {
         moments(nd);
       } else {
@@ -993,15 +1013,10 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
       }
       collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, fluid && cls ? a.table[cls] : 0u, out, fluid);
       if (!fluid) collide_solid(nd, out);
-    } else if (cls == CLASS_SOLID) {
-      collide_solid(nd, out);
-    } else {
-      moments(nd);
-      collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
-    }
-    if (active) {
-      unroll<Q>([&](auto ic) { store_dev(write_at(ic), out[decltype(ic)::value], scale); });
-      store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
+      if (active) {
+        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, n, ic), out[decltype(ic)::value], scale); });
+        store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
+      }
     }
   }
   if (DIAG)
