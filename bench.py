@@ -448,6 +448,8 @@ def run_ours(args, world, rank, local):
     tag = f"step_kernel_{args.workload}{args.size}_{args.storage}"
     if args.kernel == "pipelined":
         tag = f"step_pipelined_kernel_{args.workload}{args.size}_{args.storage}"
+    elif args.streaming == "aa":
+        tag += "_aa"
     traffic = profiled_traffic(tag)
 
     # End to end through the C ABI with host buffers.
@@ -500,7 +502,7 @@ def run_ours(args, world, rank, local):
                          "bytes_per_lup": bpl,
                          "kernel": ("step_pipelined_kernel (bulk-copy row pipeline, fused stream+BC+collide)"
                                     if args.kernel == "pipelined" else
-                                    "step_kernel (direct loads, fused stream+BC+collide)")},
+                                    f"step_kernel (direct loads, fused stream+BC+collide, {args.streaming} layout)")},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
@@ -520,7 +522,7 @@ def main():
     ap.add_argument("--storage", choices=list(STORAGE_BYTES), default="f32")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--kernel", choices=["auto", "direct", "pipelined"], default="auto")
-    ap.add_argument("--streaming", choices=["shift", "aa"], default="shift")
+    ap.add_argument("--streaming", choices=["shift", "aa"], default="aa")
     ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
     ap.add_argument("--domains", type=int, default=4096)
     ap.add_argument("--batch-cap", type=int, default=20000)
