@@ -338,6 +338,104 @@ lbmc_status lbmc_lattice_tables(int lattice, int *e, double *w, int *opp, int *m
 /* Message of the last error on the calling thread ("" if none). */
 const char *lbmc_last_error(void);
 
+/* ------------------------------------------------------------------------
+ * Run control: the reference's front end (input file, model builder, output
+ * handler, driver loop) around the step.
+ * ------------------------------------------------------------------------ */
+
+/* Stored macros of one node (rho, u_x, u_y, u_z) as of the last
+ * LBMC_STORE_MACROS step: the single-node read of screen_mess
+ * (LBM-C/index.cu:412-439). */
+lbmc_status lbmc_probe(lbmc_handle *h, long long node, double out[4]);
+
+#define LBMC_PATH_MAX 256
+
+/* Everything an input file sets.  Replaces the reference's DomainConstant
+ * fields, Timing, OutputController and ProjectStrings as filled by
+ * InfileReader (LBM-C/infile_reader.cu:45-226, LBM-C/data_types.cuh:57-79). */
+typedef struct lbmc_run_config {
+  lbmc_config cfg;                  /* Tau, TauMRT, Lx/Ly/Lz, C_smag, ColType, Force,
+                                       MicroBC, MacroBC, Tolerance, Init, DeltaX, DeltaT */
+  char project_name[LBMC_PATH_MAX]; /* ProjName */
+  char domain_file[LBMC_PATH_MAX];  /* DomainFile */
+  char output_file[LBMC_PATH_MAX];  /* OutputFile */
+  int max_t;                        /* MaxT: steps */
+  int file_out;                     /* FileOut: output every n steps (0 = never) */
+  int screen_mes;                   /* ScreenMes: screen line every n steps */
+  int steady_check;                 /* SteadyCheck: residual every n steps */
+  int output_u[3], output_rho, output_pressure; /* OutputVars */
+  int screen_node[3];               /* ScreenNode */
+  int interactive;                  /* Interactive (read and reported; no pauses) */
+  int lz_given;                     /* an Lz line was read */
+  int lattice_given;                /* a Lattice line (D2Q9 / D3Q15) was read */
+  int tau_mrt_count;                /* values read from TauMRT */
+} lbmc_run_config;
+
+/* Reads an input file the way InfileReader does: for each line, the text
+ * before '#' is matched against the keys in the reference's order by
+ * substring (ProjName, DomainFile, OutputFile, TauMRT, Tau, Lx, Ly, Lz,
+ * DeltaX, DeltaT, C_smag, ColType, Force, MicroBC, MacroBC, Tolerance, Init,
+ * MaxT, FileOut, ScreenMes, SteadyCheck, OutputVars, ScreenNode,
+ * Interactive); the first token is the name, the values follow.  Extension:
+ * a "Lattice D2Q9|D3Q15" line; without it the lattice is D3Q15 when an Lz
+ * line gives Lz > 1, else D2Q9 (the reference fixes DIM at compile time and
+ * ignores Lz in 2-D builds).  `echo` (may be NULL) receives the report the
+ * reference prints, "name = value" per line. */
+lbmc_status lbmc_read_input(const char *path, lbmc_run_config *rc, char *echo, size_t echo_bytes);
+
+/* Host arrays of a model, read from the domain directory named by
+ * DomainFile: one NumPy .npy file per field, named as the reference's CGNS
+ * fields (ModelBuilder::variable_loader, LBM-C/model_builder.cu:173-231):
+ * Porosity; ForceX/ForceY/ForceZ when Force; MicroBC when MicroBC; MacroBC,
+ * VelocityX/Y/Z and Rho when MacroBC; VelocityX/Y/Z and Rho for Init 1
+ * (equilibrium); Populations (Q x N) for Init 2.  Arrays are float64,
+ * float32, int32 or int64, C order, N = Lx Ly Lz elements in the node order
+ * x + Lx (y + Ly z).  A missing Porosity file means all fluid. */
+typedef struct lbmc_model lbmc_model;
+lbmc_status lbmc_model_build(const lbmc_run_config *rc, lbmc_model **out);
+/* Pointers into the model's arrays, valid until lbmc_model_free. */
+lbmc_status lbmc_model_domain(const lbmc_model *m, lbmc_domain *dom);
+void lbmc_model_free(lbmc_model *m);
+
+/* Solution output with the structure of the reference's CGNS output
+ * (CGNSOutputHandler, LBM-C/cgns/cgns_output_handler.cu:62-293): base
+ * "Base", structured zone "LBM-C Output Data" with an (L+1)^dim vertex grid
+ * (RealSingle CoordinateX/Y/Z), one cell-centred FlowSolution "Solution @
+ * Time = N" per output with RealDouble fields, and the iteration values and
+ * FlowSolutionPointers of BaseIterativeData / ZoneIterativeData.  No CGNS
+ * library is available to this build, so the tree is written as a
+ * directory: index.json (the tree), GridCoordinates/Coordinate?.npy and
+ * "Solution @ Time = N"/<field>.npy. */
+typedef struct lbmc_output lbmc_output;
+lbmc_status lbmc_output_open(const char *path, int dim, const int length[3], lbmc_output **out);
+lbmc_status lbmc_output_append(lbmc_output *o, long long step, int nfields, const double *const *data,
+                               const char *const *labels);
+/* Writes the iterative data and closes. */
+lbmc_status lbmc_output_close(lbmc_output *o);
+
+/* Result of a driver run. */
+typedef struct lbmc_run_result {
+  long long steps;     /* steps taken */
+  int steady;          /* stopped by the steady-state test */
+  int nonfinite;       /* stopped on a non-finite state (the reference exits with 1) */
+  int outputs;         /* solutions written */
+  double residual[3];  /* the last NUM_RESIDS residuals */
+  double seconds;      /* wall clock of the time loop */
+} lbmc_run_result;
+
+/* The reference's main() (LBM-C/index.cu:61-153): read the input file,
+ * build the model, run MaxT steps with output every FileOut steps, a screen
+ * line every ScreenMes steps and the steady-state test every SteadyCheck
+ * steps (residual = |KE - KE_prev| / SteadyCheck / KE from the fused FP64
+ * kinetic-energy sum; stop when the last three are below Tolerance, with an
+ * output; on a non-finite state write an output and stop).  Macros are
+ * stored only on the steps that use them (the reference stores on nearly
+ * every step when SteadyCheck > 0, defect Q7).  `cfg_overrides` (may be
+ * NULL) supplies storage, streaming, device and kernel in place of the
+ * defaults.  quiet = 1 suppresses the screen report. */
+lbmc_status lbmc_run(const char *input_path, const lbmc_config *cfg_overrides, int quiet,
+                     lbmc_run_result *res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -647,6 +647,28 @@ extern "C" lbmc_status lbmc_fetch(lbmc_handle *h, int field, void *dst, size_t b
   }
 }
 
+extern "C" lbmc_status lbmc_probe(lbmc_handle *h, long long node, double out[4]) {
+  if (!h || !out) return fail(LBMC_ERR_INVALID_ARG, "lbmc_probe: NULL argument");
+  const DeviceState &d = h->ds;
+  if (node < 0 || node >= d.n) return fail(LBMC_ERR_INVALID_ARG, "lbmc_probe: node %lld outside the domain", node);
+  CK(cudaSetDevice(h->cfg.device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(h->stream), "lbmc_probe");
+  const void *src[4] = {d.rho, d.u[0], d.u[1], d.dim == 3 ? d.u[2] : nullptr};
+  for (int k = 0; k < 4; k++) {
+    out[k] = 0.0;
+    if (!src[k]) continue;
+    if (h->ops->csize == 8) {
+      CK(cudaMemcpy(&out[k], static_cast<const double *>(src[k]) + node, 8, cudaMemcpyDeviceToHost), "lbmc_probe");
+    } else {
+      float v = 0.f;
+      CK(cudaMemcpy(&v, static_cast<const float *>(src[k]) + node, 4, cudaMemcpyDeviceToHost), "lbmc_probe");
+      out[k] = v;
+    }
+  }
+  out[0] += 1.0;  // stored as rho - 1
+  return LBMC_OK;
+}
+
 extern "C" lbmc_status lbmc_destroy(lbmc_handle *h) {
   if (!h) return LBMC_OK;
   cudaSetDevice(h->cfg.device);

@@ -76,6 +76,26 @@ class LbmcError(RuntimeError):
 _lib = None
 
 
+PATH_MAX = 256
+
+
+class RunConfig(ctypes.Structure):
+    """lbmc_run_config: what an input file sets (include/lbmc.h)."""
+    _fields_ = [("cfg", Config), ("project_name", ctypes.c_char * PATH_MAX),
+                ("domain_file", ctypes.c_char * PATH_MAX), ("output_file", ctypes.c_char * PATH_MAX),
+                ("max_t", ctypes.c_int), ("file_out", ctypes.c_int), ("screen_mes", ctypes.c_int),
+                ("steady_check", ctypes.c_int), ("output_u", ctypes.c_int * 3),
+                ("output_rho", ctypes.c_int), ("output_pressure", ctypes.c_int),
+                ("screen_node", ctypes.c_int * 3), ("interactive", ctypes.c_int),
+                ("lz_given", ctypes.c_int), ("lattice_given", ctypes.c_int),
+                ("tau_mrt_count", ctypes.c_int)]
+
+
+class RunResult(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("steady", ctypes.c_int), ("nonfinite", ctypes.c_int),
+                ("outputs", ctypes.c_int), ("residual", ctypes.c_double * 3), ("seconds", ctypes.c_double)]
+
+
 def library() -> ctypes.CDLL:
     """The in-tree liblbmc.so (raises if it has not been built)."""
     global _lib
@@ -106,9 +126,23 @@ def library() -> ctypes.CDLL:
         lib.lbmc_macro_sums_noalloc.argtypes = [ctypes.c_int, _P, _P, _P, _P, ctypes.c_longlong,
                                                 _P, _P]
         lib.lbmc_macro_sums_noalloc.restype = ctypes.c_int
+        lib.lbmc_probe.argtypes = [_P, ctypes.c_longlong, _P]
+        lib.lbmc_read_input.argtypes = [ctypes.c_char_p, ctypes.POINTER(RunConfig), ctypes.c_char_p,
+                                        ctypes.c_size_t]
+        lib.lbmc_model_build.argtypes = [ctypes.POINTER(RunConfig), ctypes.POINTER(_P)]
+        lib.lbmc_model_domain.argtypes = [_P, ctypes.POINTER(Domain)]
+        lib.lbmc_model_free.argtypes = [_P]
+        lib.lbmc_model_free.restype = None
+        lib.lbmc_output_open.argtypes = [ctypes.c_char_p, ctypes.c_int, _P, ctypes.POINTER(_P)]
+        lib.lbmc_output_append.argtypes = [_P, ctypes.c_longlong, ctypes.c_int, _P, _P]
+        lib.lbmc_output_close.argtypes = [_P]
+        lib.lbmc_run.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config), ctypes.c_int,
+                                 ctypes.POINTER(RunResult)]
         for name in ("lbmc_config_default", "lbmc_validate", "lbmc_init", "lbmc_iterate",
                      "lbmc_fetch", "lbmc_destroy", "lbmc_get_step", "lbmc_set_stream",
-                     "lbmc_synchronize", "lbmc_classify", "lbmc_lattice_tables"):
+                     "lbmc_synchronize", "lbmc_classify", "lbmc_lattice_tables", "lbmc_probe",
+                     "lbmc_read_input", "lbmc_model_build", "lbmc_model_domain", "lbmc_output_open",
+                     "lbmc_output_append", "lbmc_output_close", "lbmc_run"):
             getattr(lib, name).restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -493,3 +527,50 @@ class Mlp:
             self.close()
         except Exception:
             pass
+
+
+# ----------------------------------------------------------- run control
+
+def read_input(path):
+    """lbmc_read_input: (RunConfig, the reader's report)."""
+    rc = RunConfig()
+    echo = ctypes.create_string_buffer(1 << 16)
+    check(library().lbmc_read_input(os.fsencode(path), ctypes.byref(rc), echo, len(echo)))
+    return rc, echo.value.decode()
+
+
+def run(path, storage=F32, streaming=STREAM_AA, device=0, quiet=True):
+    """lbmc_run: the reference's driver loop on an input file; returns
+    (status, RunResult).  LBMC_ERR_NAN is returned, not raised."""
+    ov = Config()
+    check(library().lbmc_config_default(ctypes.byref(ov), D2Q9))
+    ov.storage = STORAGE_IDS.get(storage, storage)
+    ov.streaming = streaming
+    ov.device = device
+    res = RunResult()
+    st = library().lbmc_run(os.fsencode(path), ctypes.byref(ov), int(quiet), ctypes.byref(res))
+    if st not in (OK, ERR_NAN):
+        check(st)
+    return st, res
+
+
+class Output:
+    """lbmc_output_*: the CGNS-structured solution writer."""
+
+    def __init__(self, path, dim, length):
+        h = _P()
+        L = (ctypes.c_int * 3)(*(list(length) + [1] * (3 - len(length))))
+        check(library().lbmc_output_open(os.fsencode(path), dim, L, ctypes.byref(h)))
+        self.h = h
+
+    def append(self, step, fields):
+        """fields: {label: float64 array of N values}."""
+        arrs = [np.ascontiguousarray(v, np.float64) for v in fields.values()]
+        data = (_P * len(arrs))(*[a.ctypes.data for a in arrs])
+        labels = (ctypes.c_char_p * len(arrs))(*[k.encode() for k in fields])
+        check(library().lbmc_output_append(self.h, step, len(arrs), data, labels))
+
+    def close(self):
+        if self.h:
+            check(library().lbmc_output_close(self.h))
+            self.h = None
