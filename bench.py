@@ -181,6 +181,7 @@ WORKLOAD_METRIC = {
     "porous": "GLUPS (D3Q15 MRT porous {n}^3 fused step)",
     "tgv": "GLUPS (D3Q15 BGK+Smagorinsky Taylor-Green {n}^3 fused step)",
     "poiseuille": "GLUPS (D2Q9 BGK+Guo Poiseuille 128x64 fused step)",
+    "closure": "GLUPS (D3Q15 BGK+Guo {n}^3 step with the learned subgrid closure)",
 }
 
 
@@ -190,6 +191,8 @@ def build_workload(args):
         return workloads.taylor_green(args.size)
     if args.workload == "poiseuille":
         return workloads.poiseuille_channel()
+    if args.workload == "closure":
+        return workloads.forced_box(args.size)
     L = (args.size, args.size, args.size)
     return workloads.porous_spheres(L)
 
@@ -419,6 +422,13 @@ def run_ours(args, world, rank, local):
     streaming = lbmc.STREAM_AA if args.streaming == "aa" else lbmc.STREAM_SHIFT
     eng = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel, streaming=streaming)
     lbmc.check(lbmc.library().lbmc_set_stream(eng.h, stream.cuda_stream))
+    mlp = None
+    if args.workload == "closure":
+        # The network's cost does not depend on its weights: a seeded
+        # network with an open input range, so every node evaluates it.
+        mlp = lbmc.Mlp(seed=1, device=local)
+        mlp.set_normalization(np.zeros(6), np.full(6, 10.0), target_scale=1e-5)
+        mlp.attach(eng, iterations=args.closure_passes)
     # warm-up
     eng.iterate(args.warmup, lbmc.SYNC)
     dist_barrier(world, device)
@@ -463,6 +473,8 @@ def run_ours(args, world, rank, local):
             t = time.perf_counter()
             e = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel,
                                      streaming=streaming)
+            if mlp is not None:
+                mlp.attach(e, iterations=args.closure_passes)
             e.iterate(E2E_STEPS, lbmc.STORE_MACROS | lbmc.SYNC)
             e.rho()
             e.u()
@@ -502,7 +514,9 @@ def run_ours(args, world, rank, local):
                          "bytes_per_lup": bpl,
                          "kernel": ("step_pipelined_kernel (bulk-copy row pipeline, fused stream+BC+collide)"
                                     if args.kernel == "pipelined" else
-                                    f"step_kernel (direct loads, fused stream+BC+collide, {args.streaming} layout)")},
+                                    f"step_kernel (direct loads, fused stream+BC+collide, {args.streaming} layout)"
+                                    + (f", learned closure {args.closure_passes} pass(es) on the tensor cores:"
+                                       " SFU/issue-bound, not HBM-bound" if mlp is not None else ""))},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
@@ -523,6 +537,7 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--kernel", choices=["auto", "direct", "pipelined"], default="auto")
     ap.add_argument("--streaming", choices=["shift", "aa"], default="aa")
+    ap.add_argument("--closure-passes", type=int, default=1)
     ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
     ap.add_argument("--domains", type=int, default=4096)
     ap.add_argument("--batch-cap", type=int, default=20000)

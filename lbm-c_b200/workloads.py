@@ -150,6 +150,17 @@ def taylor_green(L=256, u0=0.05, re=1600.0, c_smag=0.1) -> Workload:
                     params=dict(nu=nu, u0=u0, re=re, ell=ell))
 
 
+def forced_box(L=128, tau=0.5025, amp=1.6e-5, c_smag=0.1, seed=1) -> Workload:
+    """Periodic D3Q15 BGK box driven by a static solenoidal Guo force of
+    random Fourier modes |k| <= 2 (the closure study's coarse grid);
+    Smagorinsky C_s = c_smag where a learned closure's inputs leave its
+    range."""
+    import closure
+    force = closure.fourier_force(L, amp, 2, seed)
+    return Workload("forced_box_d3q15_bgk", "d3q15", (L, L, L), tau, 0, c_smag=c_smag, forcing=True,
+                    arrays=dict(force=force), params=dict(amp=amp, seed=seed))
+
+
 def engine_for(lbmc, w: Workload, storage="f32", **kw):
     """lbmc.Engine for a workload (lbmc is the binding module)."""
     a = w.arrays
