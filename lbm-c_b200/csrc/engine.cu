@@ -18,7 +18,10 @@
 #include <cstring>
 #include <map>
 #include <new>
+#include <climits>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lbmc.h"
@@ -85,6 +88,25 @@ const LatticeStorageOps *select_ops(int lattice, int storage) {
 
 bool is_sf_code(int lattice, int code) {
   return lattice == LBMC_D2Q9 ? (code >= 5 && code <= 8) : (code >= 7 && code <= 12);
+}
+
+// Runs body(begin, end, chunk) over [0, n) in contiguous chunks on the
+// host's cores (serially for small n); chunk c covers an increasing range,
+// so per-chunk results concatenated in chunk order are in node order.
+template <class F>
+int parallel_for(long long n, F body) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int t = (int)(hw == 0 ? 1 : (hw > 32 ? 32 : hw));
+  if (n < (1LL << 20)) t = 1;
+  const long long per = (n + t - 1) / t;
+  std::vector<std::thread> pool;
+  for (int c = 1; c < t; c++) {
+    const long long b = c * per, e = std::min(n, b + per);
+    if (b < e) pool.emplace_back(body, b, e, c);
+  }
+  body(0LL, std::min(n, per), 0);
+  for (auto &th : pool) th.join();
+  return t;
 }
 
 // Host-side packing of the per-node inputs.
@@ -183,74 +205,143 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     return fail(LBMC_ERR_INVALID_ARG, "macro_bc is on but domain.macro_bc is NULL");
   if (cfg->micro_bc && !dom->micro_bc)
     return fail(LBMC_ERR_INVALID_ARG, "micro_bc is on but domain.micro_bc is NULL");
-  const int q = lattice_q(cfg->lattice);
-  bool needs_rho = false;
-  for (long long k = 0; k < n; k++) {
+  // Per-node checks; the first failing node in node order is reported.
+  // Returns 0 if node k is fine, else writes the message.
+  const bool have_u = dom->u[0] && dom->u[1] && (dim == 2 || dom->u[2]);
+  auto check_node = [&](long long k, bool &needs_rho, char *msg, size_t len) -> bool {
     const double B = dom->geometry ? dom->geometry[k] : 0.0;
-    if (!std::isfinite(B)) return fail(LBMC_ERR_INVALID_ARG, "Porosity at node %lld is not finite", k);
-    if (B >= 1) continue;
+    if (!std::isfinite(B)) {
+      snprintf(msg, len, "Porosity at node %lld is not finite", k);
+      return false;
+    }
+    if (B >= 1) return true;
     if (cfg->macro_bc) {
       const int c = dom->macro_bc[k];
-      if (c < 0 || c > 15) return fail(LBMC_ERR_INVALID_ARG, "MacroBC code %d at node %lld is outside 0..15", c, k);
+      if (c < 0 || c > 15) {
+        snprintf(msg, len, "MacroBC code %d at node %lld is outside 0..15", c, k);
+        return false;
+      }
       if (macro_mask(c) & 0x8) needs_rho = true;
-      if ((macro_mask(c) & 0x7) && !(dom->u[0] && dom->u[1] && (dim == 2 || dom->u[2])))
-        return fail(LBMC_ERR_INVALID_ARG, "MacroBC code %d needs the velocity fields", c);
+      if ((macro_mask(c) & 0x7) && !have_u) {
+        snprintf(msg, len, "MacroBC code %d needs the velocity fields", c);
+        return false;
+      }
     }
     if (cfg->micro_bc) {
       const int c = dom->micro_bc[k];
       const int maxc = cfg->lattice == LBMC_D2Q9 ? 8 : 12;
-      if (c < 0 || c > maxc)
-        return fail(LBMC_ERR_INVALID_ARG, "MicroBC code %d at node %lld is outside 0..%d", c, k, maxc);
+      if (c < 0 || c > maxc) {
+        snprintf(msg, len, "MicroBC code %d at node %lld is outside 0..%d", c, k, maxc);
+        return false;
+      }
       // micro_bc.cuh:7-8 leaves D2Q9 codes 3 and 4 as NULL entries.
-      if (cfg->lattice == LBMC_D2Q9 && (c == 3 || c == 4))
-        return fail(LBMC_ERR_INVALID_ARG, "MicroBC code %d is undefined for D2Q9 (node %lld)", c, k);
+      if (cfg->lattice == LBMC_D2Q9 && (c == 3 || c == 4)) {
+        snprintf(msg, len, "MicroBC code %d is undefined for D2Q9 (node %lld)", c, k);
+        return false;
+      }
     }
+    return true;
+  };
+  struct Chunk {
+    long long bad = LLONG_MAX;
+    bool needs_rho = false;
+  };
+  std::vector<Chunk> chunks(32);
+  parallel_for(n, [&](long long b, long long e, int c) {
+    char msg[160];
+    for (long long k = b; k < e; k++)
+      if (!check_node(k, chunks[c].needs_rho, msg, sizeof(msg))) {
+        chunks[c].bad = k;
+        break;
+      }
+  });
+  bool needs_rho = false;
+  long long bad = LLONG_MAX;
+  for (const Chunk &c : chunks) {
+    needs_rho = needs_rho || c.needs_rho;
+    bad = std::min(bad, c.bad);
+  }
+  if (bad != LLONG_MAX) {
+    char msg[160];
+    bool unused = false;
+    check_node(bad, unused, msg, sizeof(msg));
+    return fail(LBMC_ERR_INVALID_ARG, "%s", msg);
   }
   if (needs_rho && !dom->rho) return fail(LBMC_ERR_INVALID_ARG, "a MacroBC code prescribes rho but domain.rho is NULL");
-  (void)q;
   return LBMC_OK;
 }
 
 // Packs Porosity / MacroBC / MicroBC into class bytes (host only, no GPU).
+// Class ids >= 2 go to the distinct (MacroBC, MicroBC, partial) entries in
+// the order of their first node; the pass runs on the host's cores.
 static lbmc_status build_classes(const lbmc_config *cfg, const lbmc_domain *dom, long long n,
                                  HostClasses &hc) {
-  hc.cls.assign(n, 0);
+  hc.cls.resize(n);
   memset(hc.table, 0, sizeof(hc.table));
-  std::map<unsigned, int> ids;
   const bool blend = cfg->collision_type == LBMC_NTPOR || cfg->collision_type == LBMC_MRTPOR;
-  const int L0 = cfg->length[0], L1 = cfg->length[1];
-  for (long long k = 0; k < n; k++) {
-    const double B = dom->geometry ? dom->geometry[k] : 0.0;
-    if (B >= 1) {  // LBM-C/solver.cu:67-72
-      hc.cls[k] = CLASS_SOLID;
-      continue;
-    }
-    const int macro = cfg->macro_bc ? dom->macro_bc[k] : 0;
-    const int micro = cfg->micro_bc ? dom->micro_bc[k] : 0;
-    const bool partial = blend && B != 0.0;
-    const unsigned entry = (unsigned)macro | ((unsigned)micro << ENTRY_MICRO_SHIFT) | (partial ? ENTRY_PARTIAL : 0u);
-    if (partial) hc.any_partial = true;
-    if (micro && is_sf_code(cfg->lattice, micro)) {
-      const int face = cfg->lattice == LBMC_D2Q9 ? micro - 5 : micro - 7;
-      hc.sf_nodes.push_back((int)k);
-      hc.sf_face.push_back((uint8_t)face);
-    }
-    if (!entry) continue;
-    auto it = ids.find(entry);
-    int id;
-    if (it == ids.end()) {
-      if (hc.nclasses >= 256)
-        return fail(LBMC_ERR_UNSUPPORTED, "more than 254 distinct (MacroBC, MicroBC, partial) combinations");
-      id = hc.nclasses++;
-      ids[entry] = id;
-      hc.table[id] = (uint16_t)entry;
-    } else {
-      id = it->second;
-    }
-    hc.cls[k] = (uint8_t)id;
+  constexpr int KEYS = 512;            // macro (4 bits) | micro << 4 (4 bits) | partial << 8
+  constexpr uint16_t SOLID_KEY = 0xFFFF;
+  std::unique_ptr<uint16_t[]> key(new uint16_t[n]);
+  struct Chunk {
+    long long first[KEYS];
+    bool any_partial = false;
+    std::vector<int> sf_nodes;
+    std::vector<uint8_t> sf_face;
+  };
+  std::vector<std::unique_ptr<Chunk>> chunks(32);
+  for (auto &c : chunks) {
+    c.reset(new Chunk());
+    for (int k = 0; k < KEYS; k++) c->first[k] = LLONG_MAX;
   }
-  (void)L0;
-  (void)L1;
+  parallel_for(n, [&](long long b, long long e, int ci) {
+    Chunk &c = *chunks[ci];
+    for (long long k = b; k < e; k++) {
+      const double B = dom->geometry ? dom->geometry[k] : 0.0;
+      if (B >= 1) {  // LBM-C/solver.cu:67-72
+        key[k] = SOLID_KEY;
+        continue;
+      }
+      const int macro = cfg->macro_bc ? dom->macro_bc[k] : 0;
+      const int micro = cfg->micro_bc ? dom->micro_bc[k] : 0;
+      const bool partial = blend && B != 0.0;
+      const unsigned entry = (unsigned)macro | ((unsigned)micro << ENTRY_MICRO_SHIFT) | (partial ? ENTRY_PARTIAL : 0u);
+      if (partial) c.any_partial = true;
+      if (micro && is_sf_code(cfg->lattice, micro)) {
+        c.sf_nodes.push_back((int)k);
+        c.sf_face.push_back((uint8_t)(cfg->lattice == LBMC_D2Q9 ? micro - 5 : micro - 7));
+      }
+      key[k] = (uint16_t)entry;
+      if (entry && c.first[entry] == LLONG_MAX) c.first[entry] = k;
+    }
+  });
+  // Ids by first appearance, as a sequential scan would give them.
+  std::vector<std::pair<long long, int>> order;
+  for (int e = 1; e < KEYS; e++) {
+    long long f = LLONG_MAX;
+    for (auto &c : chunks) f = std::min(f, c->first[e]);
+    if (f != LLONG_MAX) order.push_back({f, e});
+  }
+  std::sort(order.begin(), order.end());
+  if ((int)order.size() > 254)
+    return fail(LBMC_ERR_UNSUPPORTED, "more than 254 distinct (MacroBC, MicroBC, partial) combinations");
+  uint8_t id_of[KEYS] = {0};
+  hc.nclasses = 2;
+  for (auto &o : order) {
+    id_of[o.second] = (uint8_t)hc.nclasses;
+    hc.table[hc.nclasses++] = (uint16_t)o.second;
+  }
+  parallel_for(n, [&](long long b, long long e, int) {
+    for (long long k = b; k < e; k++)
+      hc.cls[k] = key[k] == SOLID_KEY ? (uint8_t)CLASS_SOLID : id_of[key[k]];
+  });
+  hc.any_partial = false;
+  hc.sf_nodes.clear();
+  hc.sf_face.clear();
+  for (auto &c : chunks) {
+    hc.any_partial = hc.any_partial || c->any_partial;
+    hc.sf_nodes.insert(hc.sf_nodes.end(), c->sf_nodes.begin(), c->sf_nodes.end());
+    hc.sf_face.insert(hc.sf_face.end(), c->sf_face.begin(), c->sf_face.end());
+  }
   return LBMC_OK;
 }
 
@@ -297,18 +388,23 @@ static lbmc_status dev_alloc(lbmc_handle *h, T **p, size_t bytes, const char *wh
   return LBMC_OK;
 }
 
-// Uploads N doubles as the compute type (float or double).
+// Uploads N doubles as the compute type (float or double), converting on
+// the host's cores.
 static lbmc_status upload_compute(lbmc_handle *h, void *dst, const double *src, long long n,
                                   double offset, double fill) {
   const int cs = h->ops->csize;
   if (cs == 8) {
-    std::vector<double> tmp(n);
-    for (long long k = 0; k < n; k++) tmp[k] = src ? src[k] + offset : fill;
-    CK(cudaMemcpy(dst, tmp.data(), n * 8, cudaMemcpyHostToDevice), "upload field");
+    std::unique_ptr<double[]> tmp(new double[n]);
+    parallel_for(n, [&](long long b, long long e, int) {
+      for (long long k = b; k < e; k++) tmp[k] = src ? src[k] + offset : fill;
+    });
+    CK(cudaMemcpy(dst, tmp.get(), n * 8, cudaMemcpyHostToDevice), "upload field");
   } else {
-    std::vector<float> tmp(n);
-    for (long long k = 0; k < n; k++) tmp[k] = (float)(src ? src[k] + offset : fill);
-    CK(cudaMemcpy(dst, tmp.data(), n * 4, cudaMemcpyHostToDevice), "upload field");
+    std::unique_ptr<float[]> tmp(new float[n]);
+    parallel_for(n, [&](long long b, long long e, int) {
+      for (long long k = b; k < e; k++) tmp[k] = (float)(src ? src[k] + offset : fill);
+    });
+    CK(cudaMemcpy(dst, tmp.get(), n * 4, cudaMemcpyHostToDevice), "upload field");
   }
   return LBMC_OK;
 }
@@ -485,29 +581,32 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   } else {
     double *tmp = nullptr;
     TRYCUDA(cudaMalloc(&tmp, sizeof(double) * n), "init staging");
-    std::vector<double> host(n);
+    std::vector<double> host(cfg->init_type == LBMC_INIT_F ? 0 : n);
     lbmc_status s2 = LBMC_OK;
     for (int i = 0; i < q && s2 == LBMC_OK; i++) {
+      const double *src = host.data();
       if (cfg->init_type == LBMC_INIT_F) {
-        memcpy(host.data(), dom->f + (size_t)i * n, sizeof(double) * n);
+        src = dom->f + (size_t)i * n;  // the caller's array, valid for the whole call
       } else {
         // f_eq(rho, u) of collision.cu:58.
         const double w = lattice_w(d.lattice, i);
-        for (long long k = 0; k < n; k++) {
-          const double rho = dom->rho ? dom->rho[k] : 1.0;
-          double u[3] = {0, 0, 0}, usq = 0, eu = 0;
-          for (int c = 0; c < d.dim; c++) {
-            u[c] = dom->u[c] ? dom->u[c][k] : 0.0;
-            usq += u[c] * u[c];
-            eu += lattice_e(d.lattice, c, i) * u[c];
+        parallel_for(n, [&](long long b, long long e, int) {
+          for (long long k = b; k < e; k++) {
+            const double rho = dom->rho ? dom->rho[k] : 1.0;
+            double u[3] = {0, 0, 0}, usq = 0, eu = 0;
+            for (int c = 0; c < d.dim; c++) {
+              u[c] = dom->u[c] ? dom->u[c][k] : 0.0;
+              usq += u[c] * u[c];
+              eu += lattice_e(d.lattice, c, i) * u[c];
+            }
+            eu *= 3.0;
+            host[k] = rho * w * (1.0 + eu + 0.5 * eu * eu - 1.5 * usq);
           }
-          eu *= 3.0;
-          host[k] = rho * w * (1.0 + eu + 0.5 * eu * eu - 1.5 * usq);
-        }
+        });
       }
       // Ordered on the handle's stream: a pageable cudaMemcpy may return
       // before its DMA lands, and the non-blocking stream would not wait.
-      cudaError_t e = cudaMemcpyAsync(tmp, host.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
+      cudaError_t e = cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream);
       if (e == cudaSuccess) e = h->ops->upload_population(d, 0, i, tmp, h->stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
       if (e != cudaSuccess) s2 = cuda_fail(e, "upload initial populations");
@@ -578,11 +677,15 @@ static lbmc_status fetch_compute(lbmc_handle *h, const void *src, double *dst, l
   if (h->ops->csize == 8) {
     CK(cudaMemcpy(dst, src, n * 8, cudaMemcpyDeviceToHost), "fetch field");
     if (offset != 0)
-      for (long long k = 0; k < n; k++) dst[k] += offset;
+      parallel_for(n, [&](long long b, long long e, int) {
+        for (long long k = b; k < e; k++) dst[k] += offset;
+      });
   } else {
-    std::vector<float> tmp(n);
-    CK(cudaMemcpy(tmp.data(), src, n * 4, cudaMemcpyDeviceToHost), "fetch field");
-    for (long long k = 0; k < n; k++) dst[k] = (double)tmp[k] + offset;
+    std::unique_ptr<float[]> tmp(new float[n]);
+    CK(cudaMemcpy(tmp.get(), src, n * 4, cudaMemcpyDeviceToHost), "fetch field");
+    parallel_for(n, [&](long long b, long long e, int) {
+      for (long long k = b; k < e; k++) dst[k] = (double)tmp[k] + offset;
+    });
   }
   return LBMC_OK;
 }

@@ -272,7 +272,10 @@ class Engine:
         return self._fetch(FIELD_RHO, np.empty(self.n))
 
     def u(self):
-        return np.stack([self._fetch(FIELD_U_X + d, np.empty(self.n)) for d in range(self.dim)])
+        out = np.empty((self.dim, self.n))
+        for d in range(self.dim):
+            self._fetch(FIELD_U_X + d, out[d])
+        return out
 
     def f(self):
         return self._fetch(FIELD_F, np.empty((self.q, self.n)))
