@@ -116,3 +116,15 @@ def test_init_without_device_reports_status(lbmc):
     with pytest.raises(lbmc.LbmcError) as ei:
         lbmc.Engine.from_case(case)
     assert ei.value.status == lbmc.ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("length,status", [
+    ((2048, 1024, 1025), "ERR_UNSUPPORTED"),   # over 2^31 nodes: 32-bit slot offsets
+    ((8, 70000, 2), "ERR_UNSUPPORTED"),        # Ly over 65535 grid rows
+    ((0, 4, 4), "ERR_INVALID_ARG"), ((4, -1, 4), "ERR_INVALID_ARG")])
+def test_validate_rejects_sizes(lbmc, length, status):
+    """Sizes are checked before any per-node work: no arrays are read."""
+    cfg = lbmc.make_config("d3q15", length, tau=0.8)
+    dom = lbmc.Domain()
+    st = lbmc.library().lbmc_validate(ctypes.byref(cfg), ctypes.byref(dom))
+    assert st == getattr(lbmc, status)
