@@ -249,7 +249,10 @@ typedef struct lbmc_batch_config {
   int device;
   int block_threads;    /* 0 = autotune (256/512/1024) */
   int steps_per_launch; /* 0 = autotune (check_every or 4*check_every) */
-  int reserved[8];
+  int wide_below;       /* tail phase: once fewer than this many domains stepped in HBM are
+                           still running, each step spreads them over every SM instead of one
+                           block per domain; 0 = default (half the SMs), < 0 = never */
+  int reserved[7];
 } lbmc_batch_config;
 
 typedef struct lbmc_batch_domain {

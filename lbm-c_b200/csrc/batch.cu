@@ -17,6 +17,16 @@
 // (queue reset + kernel) until all domains converged or hit the step cap.  An
 // autotuner times the first launches with several block sizes and K, keeps
 // the fastest.
+//
+// Tail phase.  One block per domain leaves SMs idle once fewer HBM domains
+// are running than there are blocks, and the largest domains, which need the
+// most steps, finish last on one SM each.  When fewer than `wide_below`
+// HBM domains are still running, the host switches them to a second graph
+// whose side branch steps them one step per launch over every SM (256-node
+// tiles, batch_wide_kernel) followed by a one-thread-per-domain kernel
+// (batch_wide_finish_kernel) that applies the same convergence test and step
+// accounting as batch_kernel; the same node update runs in both phases, so
+// results do not depend on the phase a step ran in.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,6 +70,7 @@ struct BatchArgs {
   int ndomains;              // entries in order
   int *queue;                // this kernel's atomic work counter (reset before each launch)
   int *active;               // domains still running after this launch (both kernels)
+  int *active_hbm;           // of which stepped in HBM
   int steps;                 // K: steps per launch per domain
   int check;                 // C: convergence check interval
   float tol;
@@ -211,6 +222,7 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
         st.done_ns = global_ns();
       } else {
         atomicAdd(A.active, 1);
+        if (!RESIDENT) atomicAdd(A.active_hbm, 1);
       }
     }
     __syncthreads();
@@ -218,6 +230,87 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
 }
 
 __global__ void stamp_kernel(unsigned long long *out) { *out = global_ns(); }
+
+// Tail phase: one step of the listed domains, a 256-node tile per block
+// (grid-stride over the tiles).  The convergence test's block maxima go to
+// acc[domain] (non-negative floats compare as their bit patterns).
+constexpr int WIDE_THREADS = 256;
+struct WideTile {
+  int domain, first;
+};
+
+template <class S, bool BLEND>
+__global__ void __launch_bounds__(WIDE_THREADS)
+    batch_wide_kernel(const BatchArgs A, const WideTile *tiles, int ntiles, int *acc) {
+  __shared__ float sh_red[32];
+  S *pool = reinterpret_cast<S *>(A.pool);
+  StepArgs<float> a;
+  memset(&a, 0, sizeof(a));
+  a.tau = A.tau;
+  a.force_u[0] = A.force[0];
+  a.force_u[1] = A.force[1];
+  a.scale = A.scale;
+  a.inv_scale = A.inv_scale;
+  for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+    const WideTile T = tiles[ti];
+    const BatchStateDev &st = A.state[T.domain];
+    if (st.converged) continue;  // the whole block: one domain per tile
+    const BatchDomainDev D = A.dom[T.domain];
+    const int n = D.lx * D.ly;
+    const long long t = st.t;
+    const int sx = (int)(t % D.lx), sy = (int)(t % D.ly);
+    const bool save = (t % A.check) == 0;
+    const bool test = save && t >= A.check;
+    a.B = A.B + D.node_off;
+    float2 *up = A.u_prev + D.node_off;
+    const int k = T.first + (int)threadIdx.x;
+    float dmax = 0;
+    if (k < n) {
+      float ux, uy;
+      batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, k % D.lx, k / D.lx, D.lx, D.ly, sx, sy,
+                           A.cls[D.node_off + k], a, ux, uy);
+      if (test) {
+        const float2 p = up[k];
+        dmax = fmaxf(fabsf(ux - p.x), fabsf(uy - p.y));
+      }
+      if (save) up[k] = make_float2(ux, uy);
+    }
+    if (test) {
+      const float m = block_max(dmax, sh_red);
+      if (threadIdx.x == 0) atomicMax(acc + T.domain, __float_as_int(m));
+    }
+  }
+}
+
+// After each tail-phase step: per domain, the convergence test of the step
+// just taken (max |u(t) - u(t - C)| < tol), t + 1, the step cap; at the last
+// step of a launch group the domains still running are counted.
+__global__ void batch_wide_finish_kernel(const BatchArgs A, const int *wide, int nwide, int *acc, int last) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwide) return;
+  const int d = wide[i];
+  BatchStateDev &st = A.state[d];
+  if (st.converged) return;
+  long long t = st.t;
+  const bool test = (t % A.check) == 0 && t >= A.check;
+  int stop = 0;
+  if (test) {
+    const float m = __int_as_float(acc[d]);
+    acc[d] = 0;
+    st.delta_u = m;
+    stop = m < A.tol ? 1 : 0;
+  }
+  t += 1;
+  if (!stop && t >= A.max_steps) stop = 2;
+  st.t = t;
+  if (stop) {
+    st.converged = stop;
+    st.done_ns = global_ns();
+  } else if (last) {
+    atomicAdd(A.active, 1);
+    atomicAdd(A.active_hbm, 1);
+  }
+}
 
 }  // namespace
 
@@ -234,7 +327,9 @@ struct lbmc_batch {
   BatchDomainDev *dom_dev = nullptr;
   BatchStateDev *state = nullptr;
   int *order_dev = nullptr;
-  int *counters = nullptr;  // [0] resident queue, [1] HBM queue, [2] active
+  int *counters = nullptr;  // [0] resident queue, [1] HBM queue, [2] active, [3] active in HBM
+  int *acc = nullptr;       // tail phase: per-domain convergence maxima (float bits)
+  int wide_below = 0;       // tail-phase threshold (active HBM domains)
   unsigned long long *t0 = nullptr;
   cudaStream_t stream = nullptr;
   int ssize = 4;
@@ -308,6 +403,7 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
   A.ndomains = resident ? b->n_resident : b->ndomains - b->n_resident;
   A.queue = b->counters + (resident ? 0 : 1);
   A.active = b->counters + 2;
+  A.active_hbm = b->counters + 3;
   A.steps = steps;
   A.check = check;
   A.tol = (float)tol;
@@ -324,7 +420,7 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
 
 cudaError_t enqueue(lbmc_batch *b, int steps, int check, double tol, long long max_steps, int threads,
                     cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(b->counters, 0, 3 * sizeof(int), st);
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, 4 * sizeof(int), st);
   if (e != cudaSuccess) return e;
   const BatchArgs res = make_args(b, steps, check, tol, max_steps, true);
   const BatchArgs hbm = make_args(b, steps, check, tol, max_steps, false);
@@ -333,6 +429,90 @@ cudaError_t enqueue(lbmc_batch *b, int steps, int check, double tol, long long m
     case LBMC_BF16: return launch_batch<__nv_bfloat16>(b, res, hbm, threads, st);
     default: return launch_batch<float>(b, res, hbm, threads, st);
   }
+}
+
+// Tail phase: the listed HBM domains on every SM (per step: tiles, then the
+// per-domain finish), resident domains as before, in two graph branches.
+struct WideWork {
+  WideTile *tiles = nullptr;
+  int *wide = nullptr;
+  int ntiles = 0, nwide = 0, grid = 1;
+};
+
+template <class S>
+cudaError_t launch_wide(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hbm, int threads, const WideWork &w,
+                        cudaStream_t st) {
+  cudaError_t e = cudaEventRecord(b->fork, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->fork, 0);
+  if (e != cudaSuccess) return e;
+  if (res.ndomains > 0) {
+    auto kr = b->blend ? batch_kernel<S, true, true> : batch_kernel<S, false, true>;
+    kr<<<b->sms, threads, b->smem_bytes, st>>>(res);
+  }
+  auto kw = b->blend ? batch_wide_kernel<S, true> : batch_wide_kernel<S, false>;
+  for (int s = 0; s < hbm.steps; s++) {
+    kw<<<w.grid, WIDE_THREADS, 0, b->side>>>(hbm, w.tiles, w.ntiles, b->acc);
+    batch_wide_finish_kernel<<<(w.nwide + 127) / 128, 128, 0, b->side>>>(hbm, w.wide, w.nwide, b->acc,
+                                                                        s == hbm.steps - 1);
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventRecord(b->join, b->side);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->join, 0);
+  return e;
+}
+
+cudaError_t enqueue_wide(lbmc_batch *b, int steps, int check, double tol, long long max_steps, int threads,
+                         const WideWork &w, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, 4 * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const BatchArgs res = make_args(b, steps, check, tol, max_steps, true);
+  const BatchArgs hbm = make_args(b, steps, check, tol, max_steps, false);
+  switch (b->cfg.storage) {
+    case LBMC_F16: return launch_wide<__half>(b, res, hbm, threads, w, st);
+    case LBMC_BF16: return launch_wide<__nv_bfloat16>(b, res, hbm, threads, w, st);
+    default: return launch_wide<float>(b, res, hbm, threads, w, st);
+  }
+}
+
+template <class S>
+cudaError_t wide_occupancy(bool blend, int &per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, blend ? batch_wide_kernel<S, true> : batch_wide_kernel<S, false>, WIDE_THREADS, 0);
+}
+
+// The HBM domains still running, as tiles; device arrays in w (caller frees).
+cudaError_t build_wide(lbmc_batch *b, WideWork &w) {
+  std::vector<BatchStateDev> st(b->ndomains);
+  cudaError_t e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return e;
+  std::vector<WideTile> tiles;
+  std::vector<int> wide;
+  for (int d : b->order) {
+    const BatchDomainDev &D = b->dom[d];
+    if (D.resident || st[d].converged) continue;
+    wide.push_back(d);
+    const int n = D.lx * D.ly;
+    for (int first = 0; first < n; first += WIDE_THREADS) tiles.push_back({d, first});
+  }
+  w.ntiles = (int)tiles.size();
+  w.nwide = (int)wide.size();
+  e = cudaMalloc(&w.tiles, sizeof(WideTile) * std::max(1, w.ntiles));
+  if (e == cudaSuccess) e = cudaMalloc(&w.wide, sizeof(int) * std::max(1, w.nwide));
+  if (e == cudaSuccess && w.ntiles)
+    e = cudaMemcpy(w.tiles, tiles.data(), sizeof(WideTile) * w.ntiles, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && w.nwide) e = cudaMemcpy(w.wide, wide.data(), sizeof(int) * w.nwide, cudaMemcpyHostToDevice);
+  int per_sm = 0;
+  if (e == cudaSuccess) {
+    switch (b->cfg.storage) {
+      case LBMC_F16: e = wide_occupancy<__half>(b->blend, per_sm); break;
+      case LBMC_BF16: e = wide_occupancy<__nv_bfloat16>(b->blend, per_sm); break;
+      default: e = wide_occupancy<float>(b->blend, per_sm); break;
+    }
+  }
+  // Pageable copies above: make sure they landed before the side stream reads.
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  w.grid = std::max(1, std::min(w.ntiles, b->sms * std::max(1, per_sm)));
+  return e;
 }
 
 }  // namespace
@@ -418,7 +598,8 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   alloc((void **)&b->dom_dev, ndomains * sizeof(BatchDomainDev));
   alloc((void **)&b->state, ndomains * sizeof(BatchStateDev));
   alloc((void **)&b->order_dev, ndomains * sizeof(int));
-  alloc((void **)&b->counters, 3 * sizeof(int));
+  alloc((void **)&b->counters, 4 * sizeof(int));
+  alloc((void **)&b->acc, ndomains * sizeof(int));
   alloc((void **)&b->t0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(b->pool, 0, (size_t)pop * b->ssize);  // f = w (Init 0)
   if (e == cudaSuccess) e = cudaMemcpy(b->cls, cls.data(), node, cudaMemcpyHostToDevice);
@@ -427,6 +608,7 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   if (e == cudaSuccess)
     e = cudaMemcpy(b->dom_dev, b->dom.data(), ndomains * sizeof(BatchDomainDev), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(b->state, 0, ndomains * sizeof(BatchStateDev));
+  if (e == cudaSuccess) e = cudaMemset(b->acc, 0, ndomains * sizeof(int));
   if (e == cudaSuccess)
     e = cudaMemcpy(b->order_dev, b->order.data(), ndomains * sizeof(int), cudaMemcpyHostToDevice);
   // A host-to-device cudaMemcpy from pageable memory may return before its
@@ -450,6 +632,7 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   }
   b->threads = cfg->block_threads;
   b->steps = cfg->steps_per_launch;
+  b->wide_below = cfg->wide_below == 0 ? b->sms / 2 : cfg->wide_below;
   *out = b;
   return LBMC_OK;
 }
@@ -496,25 +679,52 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
     b->steps = bs;
   }
 
-  // Capture one launch (queue reset + both kernels) in a graph and replay it.
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    cudaError_t e2 = enqueue(b, b->steps, check_every, tol, max_steps, b->threads, b->stream);
-    e = cudaStreamEndCapture(b->stream, &graph);
-    if (e2 != cudaSuccess) e = e2;
+  // Capture one launch (queue reset + both kernels) in a graph and replay it;
+  // once few HBM domains remain, switch them to the tail-phase graph.
+  auto capture = [&](auto enqueue_fn, cudaGraph_t &graph, cudaGraphExec_t &exec) -> cudaError_t {
+    cudaError_t ec = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (ec != cudaSuccess) return ec;
+    cudaError_t e2 = enqueue_fn();
+    ec = cudaStreamEndCapture(b->stream, &graph);
+    if (e2 != cudaSuccess) ec = e2;
+    if (ec == cudaSuccess) ec = cudaGraphInstantiate(&exec, graph, 0);
+    return ec;
+  };
+  cudaGraph_t graph = nullptr, graph_w = nullptr;
+  cudaGraphExec_t exec = nullptr, exec_w = nullptr;
+  WideWork w;
+  bool wide = false;
+  auto go_wide = [&]() -> cudaError_t {
+    cudaError_t ew = build_wide(b, w);
+    if (ew == cudaSuccess)
+      ew = capture([&] { return enqueue_wide(b, b->steps, check_every, tol, max_steps, b->threads, w, b->stream); },
+                   graph_w, exec_w);
+    wide = ew == cudaSuccess;
+    return ew;
+  };
+  e = capture([&] { return enqueue(b, b->steps, check_every, tol, max_steps, b->threads, b->stream); }, graph, exec);
+  int counts[4] = {0, 0, 1, 0};
+  if (e == cudaSuccess && b->wide_below > 0) {
+    // Already few HBM domains running (a small batch, or after earlier runs).
+    std::vector<BatchStateDev> st(b->ndomains);
+    e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
+    int hbm_active = 0;
+    for (int d = 0; d < b->ndomains; d++) hbm_active += !b->dom[d].resident && !st[d].converged;
+    if (e == cudaSuccess && hbm_active > 0 && hbm_active < b->wide_below) e = go_wide();
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-  int active = 1;
   const long long launches_max = max_steps / std::max(1, b->steps) + 2;
-  for (long long l = 0; e == cudaSuccess && active > 0 && l < launches_max; l++) {
-    e = cudaGraphLaunch(exec, b->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&active, b->counters + 2, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+  for (long long l = 0; e == cudaSuccess && counts[2] > 0 && l < launches_max; l++) {
+    e = cudaGraphLaunch(wide ? exec_w : exec, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counts, b->counters, sizeof(counts), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess && !wide && b->wide_below > 0 && counts[3] > 0 && counts[3] < b->wide_below) e = go_wide();
   }
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
+  if (exec_w) cudaGraphExecDestroy(exec_w);
+  if (graph_w) cudaGraphDestroy(graph_w);
+  if (w.tiles) cudaFree(w.tiles);
+  if (w.wide) cudaFree(w.wide);
   if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
   if (results) {
     std::vector<BatchStateDev> st(b->ndomains);
@@ -624,7 +834,7 @@ extern "C" lbmc_status lbmc_batch_destroy(lbmc_batch *b) {
   if (!b) return LBMC_OK;
   cudaSetDevice(b->cfg.device);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  void *ptrs[] = {b->pool, b->cls, b->B, b->u_prev, b->dom_dev, b->state, b->order_dev, b->counters, b->t0};
+  void *ptrs[] = {b->pool, b->cls, b->B, b->u_prev, b->dom_dev, b->state, b->order_dev, b->counters, b->t0, b->acc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (b->stream) cudaStreamDestroy(b->stream);

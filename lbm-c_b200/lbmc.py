@@ -319,7 +319,7 @@ class BatchConfig(ctypes.Structure):
                 ("collision_type", ctypes.c_int), ("storage", ctypes.c_int),
                 ("storage_scale", ctypes.c_double), ("device", ctypes.c_int),
                 ("block_threads", ctypes.c_int), ("steps_per_launch", ctypes.c_int),
-                ("reserved", ctypes.c_int * 8)]
+                ("wide_below", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
 
 
 class BatchDomain(ctypes.Structure):
@@ -356,7 +356,8 @@ class Batch:
     """Many independent D2Q9 domains in one persistent launch (lbmc_batch_*)."""
 
     def __init__(self, geometries, tau=1.0, force=(1e-6, 0.0), collision_type=NTPOR,
-                 storage=F16, storage_scale=0.0, device=0, block_threads=0, steps_per_launch=0):
+                 storage=F16, storage_scale=0.0, device=0, block_threads=0, steps_per_launch=0,
+                 wide_below=0):
         lib = _batch_lib()
         cfg = BatchConfig()
         cfg.tau = tau
@@ -367,6 +368,7 @@ class Batch:
         cfg.device = device
         cfg.block_threads = block_threads
         cfg.steps_per_launch = steps_per_launch
+        cfg.wide_below = wide_below
         self._keep = []
         doms = (BatchDomain * len(geometries))()
         self.shapes = []
