@@ -459,8 +459,12 @@ def run_ours(args, world, rank, local):
     if args.kernel == "pipelined":
         tag = f"step_pipelined_kernel_{args.workload}{args.size}_{args.storage}"
     elif args.streaming == "aa":
-        tag += "_aa"
+        # AA runs over 64-node tiles when Lx is a multiple of 64.
+        tag += "_aa" if w.length[0] % 64 == 0 else "_aa_untiled"
     traffic = profiled_traffic(tag)
+    layout_name = args.streaming
+    if args.streaming == "aa":
+        layout_name = "tiled aa" if w.length[0] % 64 == 0 else "aa"
 
     # End to end through the C ABI with host buffers.
     e2e = None
@@ -514,7 +518,7 @@ def run_ours(args, world, rank, local):
                          "bytes_per_lup": bpl,
                          "kernel": ("step_pipelined_kernel (bulk-copy row pipeline, fused stream+BC+collide)"
                                     if args.kernel == "pipelined" else
-                                    f"step_kernel (direct loads, fused stream+BC+collide, {args.streaming} layout)"
+                                    f"step_kernel (direct loads, fused stream+BC+collide, {layout_name} layout)"
                                     + (f", learned closure {args.closure_passes} pass(es) on the tensor cores:"
                                        " SFU/issue-bound, not HBM-bound" if mlp is not None else ""))},
             "cpu_baseline": cpu,

@@ -561,6 +561,9 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     d.timeout_cycles = (long long)(khz > 0 ? khz : 2000000) * 1000LL * 2;
   }
   d.aa = cfg->streaming == LBMC_STREAM_AA ? 1 : 0;
+  // The tiled AA layout needs whole 64-node tiles along x (one direct-kernel
+  // block each); other lengths keep the plain AA layout.
+  d.tiled = d.aa && d.L[0] % lbmc::TILE == 0 ? 1 : 0;
   d.pipeline = cfg->kernel == LBMC_KERNEL_PIPELINED ? 2 : 0;
   TRYCUDA(h->ops->plan(d), "kernel planning");
   if (cfg->kernel == LBMC_KERNEL_PIPELINED && !d.use_pipeline) {

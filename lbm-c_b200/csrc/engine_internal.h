@@ -41,6 +41,7 @@ struct DeviceState {
   unsigned *error_flag;     // device word, ERROR_TIMEOUT on an expired wait
   long long timeout_cycles; // bound of every device-side wait
   int aa;                   // AA-pattern layout (else the shift layout)
+  int tiled;                // AA over 64-node tiles (Lx a multiple of 64)
   int pipeline;             // allow the bulk-copy pipelined kernel
   int use_pipeline;         // chosen by plan()
   int stages;               // shared-memory stages of the pipelined kernel

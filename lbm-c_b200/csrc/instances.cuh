@@ -25,6 +25,7 @@ struct Launchers {
       a.s[k] = d.aa ? (int)((t & 1) % d.L[k]) : (int)(t % d.L[k]);
     }
     a.aa = d.aa;
+    a.tiled = d.tiled;
     a.odd = (int)(t & 1);
     a.rho = static_cast<C *>(d.rho);
     a.sf_buf = static_cast<const C *>(d.sf_buf);
@@ -101,6 +102,10 @@ struct Launchers {
     }
     if (!d.aa)
       step_kernel<L, S, COL, FORCE, BLEND, DIAG, STREAM_SHIFT><<<grid_dim(d), block_dim(d), 0, st>>>(a);
+    else if (d.tiled && a.odd)
+      step_kernel<L, S, COL, FORCE, BLEND, DIAG, STREAM_AAT_ODD><<<grid_dim(d), block_dim(d), 0, st>>>(a);
+    else if (d.tiled)
+      step_kernel<L, S, COL, FORCE, BLEND, DIAG, STREAM_AAT_EVEN><<<grid_dim(d), block_dim(d), 0, st>>>(a);
     else if (a.odd)
       step_kernel<L, S, COL, FORCE, BLEND, DIAG, STREAM_AA_ODD><<<grid_dim(d), block_dim(d), 0, st>>>(a);
     else

@@ -164,6 +164,7 @@ struct StepArgs {
   int L[3];
   int s[3];  // shift of the current step: t mod L (AA: t mod 2, wrapped by L)
   int aa;    // AA-pattern layout (lbmc_streaming)
+  int tiled; // AA over 64-node tiles (Lx a multiple of 64)
   int odd;   // AA: the current step is odd
   int n;
   C tau;
@@ -185,11 +186,18 @@ constexpr unsigned ERROR_TIMEOUT = 1u;
 
 // ----------------------------------------------------------- index helpers
 
-__device__ __forceinline__ int wrap_sub(int x, int s, int L) {
+// Loop unrolling in functions that the host-side layout check compiles too.
+#ifdef __CUDA_ARCH__
+#define LBMC_UNROLL _Pragma("unroll")
+#else
+#define LBMC_UNROLL
+#endif
+
+__host__ __device__ __forceinline__ int wrap_sub(int x, int s, int L) {
   const int v = x - s;
   return v < 0 ? v + L : v;
 }
-__device__ __forceinline__ int wrap_add(int x, int s, int L) {
+__host__ __device__ __forceinline__ int wrap_add(int x, int s, int L) {
   const int v = x + s;
   return v >= L ? v - L : v;
 }
@@ -206,7 +214,7 @@ __host__ __device__ constexpr int sel(int e) { return e == 0 ? 0 : (e > 0 ? 1 : 
 struct Sites {
   unsigned x[3];
   unsigned row[3][3];  // [sel(e_y)][sel(e_z)] -> Lx * (y' + Ly * z')
-  __device__ __forceinline__ void init(int cx, int cy, int cz, const int *s, const int *L) {
+  __host__ __device__ __forceinline__ void init(int cx, int cy, int cz, const int *s, const int *L) {
     x[0] = cx;
     x[1] = wrap_sub(cx, s[0], L[0]);
     x[2] = wrap_add(cx, s[0], L[0]);
@@ -215,13 +223,13 @@ struct Sites {
     const unsigned zs[3] = {(unsigned)cz, (unsigned)wrap_sub(cz, s[2], L[2]),
                             (unsigned)wrap_add(cz, s[2], L[2])};
     const unsigned lx = L[0], ly = L[1];
-#pragma unroll
+LBMC_UNROLL
     for (int a = 0; a < 3; a++)
-#pragma unroll
+LBMC_UNROLL
       for (int b = 0; b < 3; b++) row[a][b] = lx * (ys[a] + ly * zs[b]);
   }
   template <class L>
-  __device__ __forceinline__ unsigned slot(int i) const {
+  __host__ __device__ __forceinline__ unsigned slot(int i) const {
     // i is a compile-time constant after unrolling, so sel() folds.
     return x[sel(L::e(0, i))] + row[sel(L::e(1, i))][sel(L::e(2, i))];
   }
@@ -238,13 +246,77 @@ struct Sites {
 // race), and the AA-odd read map is the shift map at t = 1 with the arrays
 // swapped pairwise.  The state after every step is the same as SHIFT's;
 // only where each value sits differs.
+//
+// Tiled AA (AAT, used when Lx is a multiple of 64): the same two maps over
+// a layout cut into 64-node tiles along x, tile k holding its Q population
+// arrays back to back: element (array r, slot m) sits at
+// ((m / 64) Q + r) 64 + m mod 64.  A 64-thread block of the direct kernel
+// is one tile, so at an even step a thread reaches all its values at fixed
+// offsets r 64 from one base pointer, and at an odd step a neighbour's value
+// is a block-uniform row pointer plus one of three small per-thread x
+// offsets; no per-access address arithmetic on the population pitch.
 constexpr int STREAM_SHIFT = 0, STREAM_AA_EVEN = 1, STREAM_AA_ODD = 2;
+constexpr int STREAM_AAT_EVEN = 3, STREAM_AAT_ODD = 4;
+constexpr int TILE = 64;
+static_assert(TILE == DIRECT_BLOCK, "a direct-kernel block is one tile of the tiled AA layout");
+
+// Element index of (array r, slot m) in the tiled AA layout.
+__host__ __device__ __forceinline__ long long tiled_index(int q, long long m, int r) {
+  return ((m / TILE) * q + r) * TILE + m % TILE;
+}
+
+// Tiled-AA sites of one node (x, y, z), x = 64 bx + lane: `base` is its own
+// element (array 0), x[c] the x part of the index of x' = x, x - s, x + s
+// (c = sel(e_x)) and row[a][b] the first element of row (y', z').
+struct TiledSites {
+  long long base;
+  unsigned x[3];
+  unsigned row[3][3];
+  __host__ __device__ __forceinline__ void init_even(int bx, int lane, int cy, int cz, const int *L, int q) {
+    base = ((long long)cy + (long long)L[1] * cz) * (L[0] / TILE) * q * TILE + (long long)bx * q * TILE + lane;
+  }
+  __host__ __device__ __forceinline__ void init_odd(int bx, int lane, int cy, int cz, const int *s, const int *L,
+                                                    int q) {
+    const int cx = bx * TILE + lane;
+    const int xs[3] = {cx, wrap_sub(cx, s[0], L[0]), wrap_add(cx, s[0], L[0])};
+LBMC_UNROLL
+    for (int c = 0; c < 3; c++) x[c] = (xs[c] / TILE) * q * TILE + xs[c] % TILE;
+    const int ys[3] = {cy, wrap_sub(cy, s[1], L[1]), wrap_add(cy, s[1], L[1])};
+    const int zs[3] = {cz, wrap_sub(cz, s[2], L[2]), wrap_add(cz, s[2], L[2])};
+    const unsigned rowlen = (unsigned)(L[0] / TILE) * q * TILE;
+LBMC_UNROLL
+    for (int a = 0; a < 3; a++)
+LBMC_UNROLL
+      for (int b = 0; b < 3; b++) row[a][b] = ((unsigned)ys[a] + (unsigned)L[1] * zs[b]) * rowlen;
+  }
+};
+
+// Where the direct kernel reads population I of node n (before collision)
+// and where it writes out[I], per layout.  Shared by the kernel and the
+// host-side layout check, so both see one definition.
+template <class L, int STREAM, int I, class T>
+__host__ __device__ __forceinline__ T *read_ptr(T *f, long long pitch, int n, const Sites &st,
+                                                const TiledSites &ts) {
+  if constexpr (STREAM == STREAM_AA_EVEN) return f + I * pitch + n;
+  else if constexpr (STREAM == STREAM_AA_ODD) return f + L::opp(I) * pitch + st.template slot<L>(I);
+  else if constexpr (STREAM == STREAM_AAT_EVEN) return f + ts.base + I * TILE;
+  else if constexpr (STREAM == STREAM_AAT_ODD)
+    return (f + L::opp(I) * TILE) + (ts.row[sel(L::e(1, I))][sel(L::e(2, I))] + ts.x[sel(L::e(0, I))]);
+  else return f + I * pitch + st.template slot<L>(I);
+}
+template <class L, int STREAM, int I, class T>
+__host__ __device__ __forceinline__ T *write_ptr(T *f, long long pitch, int n, const Sites &st,
+                                                 const TiledSites &ts) {
+  if constexpr (STREAM == STREAM_SHIFT) return read_ptr<L, STREAM, I>(f, pitch, n, st, ts);
+  else return read_ptr<L, STREAM, L::opp(I)>(f, pitch, n, st, ts);
+}
 
 // Array index and slot of population i of a node for the cold kernels
 // (stress-free gather, fetch, upload), from the runtime layout flags.
 template <class L, int I, class C>
-__device__ __forceinline__ long long natural_slot(const StepArgs<C> &a, const Sites &st) {
+__host__ __device__ __forceinline__ long long natural_slot(const StepArgs<C> &a, const Sites &st) {
   const int arr = (a.aa && a.odd) ? L::opp(I) : I;
+  if (a.tiled) return tiled_index(L::Q, st.template slot<L>(I), arr);
   return (long long)arr * a.pitch + st.template slot<L>(I);
 }
 
@@ -949,15 +1021,21 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
   // an AA-even step, (opp(i), slot(i)) with the t = 1 shift at an AA-odd
   // step; out[i] goes back to slot(i) (shift) or to population opp(i)'s
   // read slot (AA).
-  auto read_at = [&](S *f, const Sites &st, int n, auto ic) -> S * {
-    constexpr int i = decltype(ic)::value;
-    if constexpr (STREAM == STREAM_AA_EVEN) return f + i * a.pitch + n;
-    else if constexpr (STREAM == STREAM_AA_ODD) return f + L::opp(i) * a.pitch + st.template slot<L>(i);
-    else return f + i * a.pitch + st.template slot<L>(i);
+  auto read_at = [&](S *f, const Sites &st, const TiledSites &ts, int n, auto ic) -> S * {
+    return read_ptr<L, STREAM, decltype(ic)::value>(f, a.pitch, n, st, ts);
   };
-  auto write_at = [&](S *f, const Sites &st, int n, auto ic) -> S * {
-    if constexpr (STREAM == STREAM_SHIFT) return read_at(f, st, n, ic);
-    else return read_at(f, st, n, std::integral_constant<int, L::opp(decltype(ic)::value)>{});
+  auto write_at = [&](S *f, const Sites &st, const TiledSites &ts, int n, auto ic) -> S * {
+    return write_ptr<L, STREAM, decltype(ic)::value>(f, a.pitch, n, st, ts);
+  };
+  // The AA-even map needs only n; the others their sites (one block row per
+  // (y, z), so the row parts are uniform across the block).
+  auto init_sites = [&](Sites &st, TiledSites &ts) {
+    if constexpr (STREAM == STREAM_AAT_EVEN)
+      ts.init_even(blockIdx.x, threadIdx.x, blockIdx.y, blockIdx.z, a.L, Q);
+    else if constexpr (STREAM == STREAM_AAT_ODD)
+      ts.init_odd(blockIdx.x, threadIdx.x, blockIdx.y, blockIdx.z, a.s, a.L, Q);
+    else if constexpr (STREAM != STREAM_AA_EVEN)
+      st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
   };
   double dv[DIAG_VALUES] = {0, 0, 0, 0, 0};
   bool nonfinite = false;
@@ -966,11 +1044,12 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
     if (active) {
       const C inv_scale = a.inv_scale, scale = a.scale;
       Sites st;
-      if constexpr (STREAM != STREAM_AA_EVEN) st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
+      TiledSites ts;
+      init_sites(st, ts);
       const int n = x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z);
       S *f = reinterpret_cast<S *>(a.f);
       Node<L, C> nd;
-      unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(f, st, n, ic), inv_scale); });
+      unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(f, st, ts, n, ic), inv_scale); });
       const int cls = a.cls[n];
       C out[Q];
       if (cls == CLASS_SOLID) {
@@ -979,7 +1058,18 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
         moments(nd);
         collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
       }
-      unroll<Q>([&](auto ic) { store_dev(write_at(f, st, n, ic), out[decltype(ic)::value], scale); });
+      if constexpr (STREAM == STREAM_AAT_ODD) {
+        // The store addresses equal the load addresses.  Recomputing them
+        // from the three 32-bit x offsets is cheaper than keeping Q 64-bit
+        // pointers live across the collision, which spills 88-116 bytes at
+        // this kernel's register cap (measured: 13% slower with FP16/BF16
+        // storage).  The empty asm hides the equality from the compiler.
+        TiledSites tw = ts;
+        asm("" : "+r"(tw.x[0]), "+r"(tw.x[1]), "+r"(tw.x[2]));
+        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, tw, n, ic), out[decltype(ic)::value], scale); });
+      } else {
+        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, ts, n, ic), out[decltype(ic)::value], scale); });
+      }
       store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
     }
   } else {
@@ -992,12 +1082,13 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
     if (run) {
       const C inv_scale = a.inv_scale, scale = a.scale;
       Sites st;
+      TiledSites ts;
       const int n = active ? x + a.L[0] * ((int)blockIdx.y + a.L[1] * (int)blockIdx.z) : 0;
       S *f = reinterpret_cast<S *>(a.f);
       Node<L, C> nd;
       if (active) {
-        if constexpr (STREAM != STREAM_AA_EVEN) st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
-        unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(f, st, n, ic), inv_scale); });
+        init_sites(st, ts);
+        unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = load_dev(read_at(f, st, ts, n, ic), inv_scale); });
       } else {
         unroll<Q>([&](auto ic) { nd.g[decltype(ic)::value] = C(0); });
       }
@@ -1014,7 +1105,7 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
       collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, fluid && cls ? a.table[cls] : 0u, out, fluid);
       if (!fluid) collide_solid(nd, out);
       if (active) {
-        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, n, ic), out[decltype(ic)::value], scale); });
+        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, ts, n, ic), out[decltype(ic)::value], scale); });
         store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
       }
     }

@@ -2,7 +2,9 @@
 
 The two layouts hold the same state after every step; only the slot a
 value sits in differs (even steps read and write each node's own slots,
-odd steps its neighbours').  So every result read through the public API
+odd steps its neighbours').  AA runs in the tiled layout (64-node tiles,
+populations of a tile back to back) when Lx is a multiple of 64 and in the
+plain AA layout otherwise; both are covered.  So every result read through the public API
 must be bit-identical: populations (natural order, un-mapped by
 lbmc_fetch), stored rho/u and the FP64 diagnostic sums, after odd and
 even step counts, for every collision type, forcing, macro, Zou-He and
@@ -36,12 +38,17 @@ def run(lbmc, case, steps, storage, streaming):
         return out
 
 
+LENGTHS = {("d2q9", False): (37, 21, 1), ("d3q15", False): (19, 11, 9),
+           ("d2q9", True): (128, 9, 1), ("d3q15", True): (64, 7, 6)}
+
+
+@pytest.mark.parametrize("tiled", [False, True], ids=["plain", "tiled"])
 @pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
 @pytest.mark.parametrize("lat,ct,forcing,bc,smag", AA_COMBOS)
-def test_aa_equals_shift(lbmc, lat, ct, forcing, bc, smag, storage):
+def test_aa_equals_shift(lbmc, lat, ct, forcing, bc, smag, storage, tiled):
     if storage != "f32" and (forcing or smag or ct in (1, 2)):
         pytest.skip("storage formats are covered on the plain and MRT+partial cases")
-    length = (37, 21, 1) if lat == "d2q9" else (19, 11, 9)
+    length = LENGTHS[(lat, tiled)]
     case = make_case(lat, length, ct, forcing, solids=0.08, partial=0.15 if ct % 2 else 0.0,
                      macro="random" if bc == "random" else None,
                      micro=bc if bc in ("zh", "sf") else None, c_smag=smag, seed=7 + ct)
@@ -67,7 +74,13 @@ def test_aa_large_periodic_and_closure(lbmc):
     m = lbmc.Mlp(seed=4)
     m.set_params(0.3 * rng.standard_normal(1313))
     m.set_normalization(np.zeros(6), np.full(6, 5.0), target_scale=1e-3)
-    small = make_case("d3q15", (40, 6, 5), 0, True, solids=0.2, seed=5, uniform_force=True)
+    for length in ((40, 6, 5), (64, 6, 5)):  # plain and tiled AA layout
+        _closure_aa_vs_shift(lbmc, m, length)
+    m.close()
+
+
+def _closure_aa_vs_shift(lbmc, m, length):
+    small = make_case("d3q15", length, 0, True, solids=0.2, seed=5, uniform_force=True)
     small.c_smag = 0.1
     for storage in (lbmc.F64, lbmc.F32):
         res = []
@@ -84,7 +97,6 @@ def test_aa_large_periodic_and_closure(lbmc):
             # the compiler contracts differently: differences at the FP32
             # rounding level appear from the first odd step on.
             assert np.abs(res[0] - res[1]).max() <= 1e-7 * np.abs(res[0]).max()
-    m.close()
 
 
 def test_aa_rejects_pipelined_kernel(lbmc):

@@ -11,7 +11,9 @@ from oracle.oracle import Restatement
 pytestmark = pytest.mark.gpu
 
 TINY = [("d3q15", (1, 1, 1)), ("d3q15", (1, 7, 5)), ("d3q15", (2, 1, 3)), ("d3q15", (3, 2, 1)),
-        ("d2q9", (1, 1, 1)), ("d2q9", (1, 6, 1)), ("d2q9", (2, 2, 1)), ("d2q9", (5, 1, 1))]
+        ("d2q9", (1, 1, 1)), ("d2q9", (1, 6, 1)), ("d2q9", (2, 2, 1)), ("d2q9", (5, 1, 1)),
+        # whole 64-node tiles along x: the tiled AA layout, one tile per row
+        ("d3q15", (64, 1, 1)), ("d3q15", (64, 2, 1)), ("d3q15", (64, 1, 3)), ("d2q9", (64, 1, 1))]
 
 
 def err(a, b):
@@ -40,7 +42,9 @@ def test_degenerate_axes(lbmc, lat, length, streaming):
 @pytest.mark.parametrize("streaming", ["shift", "aa"])
 @pytest.mark.parametrize("lat,length,ct,bc", [
     ("d3q15", (65, 3, 2), 3, "zh"), ("d3q15", (130, 2, 2), 0, "random"),
-    ("d2q9", (97, 5, 1), 1, "zh"), ("d2q9", (161, 3, 1), 2, "random")])
+    ("d2q9", (97, 5, 1), 1, "zh"), ("d2q9", (161, 3, 1), 2, "random"),
+    # several tiles per row (tiled AA: x neighbours across tile edges)
+    ("d3q15", (128, 3, 2), 3, "zh"), ("d2q9", (192, 4, 1), 0, "random")])
 def test_rows_across_blocks(lbmc, lat, length, ct, bc, streaming):
     case = make_case(lat, length, ct, True, solids=0.1, partial=0.15 if ct % 2 else 0.0,
                      macro="random" if bc == "random" else None, micro="zh" if bc == "zh" else None,
