@@ -85,7 +85,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -469,7 +469,7 @@ def run_ours(args, world, rank, local):
     # End to end through the C ABI with host buffers.
     e2e = None
     if not args.no_e2e:
-        times = []
+        times, phases = [], []
         h2d = w.host_bytes()
         d2h = w.n * 8 * (1 + w.dim)
         for k in range(args.e2e_reps + 1):
@@ -479,17 +479,24 @@ def run_ours(args, world, rank, local):
                                      streaming=streaming)
             if mlp is not None:
                 mlp.attach(e, iterations=args.closure_passes)
+            t1 = time.perf_counter()
             e.iterate(E2E_STEPS, lbmc.STORE_MACROS | lbmc.SYNC)
+            t2 = time.perf_counter()
             e.rho()
             e.u()
+            t3 = time.perf_counter()
             e.close()
-            dt = time.perf_counter() - t
-            if k > 0:
-                times.append(dt)
+            t4 = time.perf_counter()
+            if k > 0:  # the first job pays for context and module loading
+                times.append(t4 - t)
+                phases.append({"init": round(t1 - t, 4), "steps": round(t2 - t1, 4),
+                               "fetch": round(t3 - t2, 4), "destroy": round(t4 - t3, 4)})
+        # The slowest job counts.
         e2e_rate, _ = aggregate_rate(w.n * E2E_STEPS, max(times), world, device)
         e2e = {"value": e2e_rate / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "job": f"lbmc_init from host arrays + {E2E_STEPS} steps + fetch rho,u + destroy"}
+               "job": f"lbmc_init from host arrays + {E2E_STEPS} steps + fetch rho,u + destroy",
+               "seconds_per_job": [round(x, 4) for x in times], "phases": phases}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -534,7 +541,9 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    # 10000 steps of the default workload take about 3 s: long enough for
+    # the clock record to hold tens of samples, short of a minute.
+    ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--storage", choices=list(STORAGE_BYTES), default="f32")

@@ -89,7 +89,9 @@ typedef enum lbmc_init_type {
 
 typedef enum lbmc_streaming {
   LBMC_STREAM_SHIFT = 0, /* in place, population i of node x at (x - t e_i) mod L */
-  LBMC_STREAM_AA = 1     /* in place, AA pattern (even/odd step index maps) */
+  LBMC_STREAM_AA = 1     /* in place, AA pattern (even/odd step index maps); over 64-node
+                            tiles when Lx is a multiple of 64 (internal: lbmc_fetch and
+                            LBMC_INIT_F always use natural order) */
 } lbmc_streaming;
 
 /* Reproduce documented reference defects exactly ("as-is" behaviour). */

@@ -562,8 +562,9 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   }
   d.aa = cfg->streaming == LBMC_STREAM_AA ? 1 : 0;
   // The tiled AA layout needs whole 64-node tiles along x (one direct-kernel
-  // block each); other lengths keep the plain AA layout.
-  d.tiled = d.aa && d.L[0] % lbmc::TILE == 0 ? 1 : 0;
+  // block each) and element indices over all Q arrays below 2^32 (its row
+  // and x offsets are 32-bit); other domains keep the plain AA layout.
+  d.tiled = d.aa && d.L[0] % lbmc::TILE == 0 && (long long)q * n < (1ll << 32) ? 1 : 0;
   d.pipeline = cfg->kernel == LBMC_KERNEL_PIPELINED ? 2 : 0;
   TRYCUDA(h->ops->plan(d), "kernel planning");
   if (cfg->kernel == LBMC_KERNEL_PIPELINED && !d.use_pipeline) {
@@ -573,7 +574,9 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
                 "and two stages of Q rows to fit in shared memory");
   }
   h->nblocks = d.nblocks;
-  TRY(dev_alloc(h, &d.partials, sizeof(double) * DIAG_VALUES * h->nblocks, "diagnostic partials"));
+  // Per-block partials of the step, then the finalize blocks' sums.
+  TRY(dev_alloc(h, &d.partials, sizeof(double) * DIAG_VALUES * (h->nblocks + FINALIZE_BLOCKS),
+                "diagnostic partials"));
   TRY(dev_alloc(h, &d.flag, sizeof(unsigned), "diagnostic flag"));
   TRY(dev_alloc(h, &h->diag_out, sizeof(double) * DIAG_VALUES, "diagnostics"));
   TRYCUDA(cudaMemset(d.flag, 0, sizeof(unsigned)), "clear flag");
@@ -625,20 +628,34 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   return LBMC_OK;
 }
 
-// Sums the per-block partials in FP64 in a fixed order (deterministic).
-__global__ void diag_finalize_kernel(const double *partials, long long nblocks, double *out) {
-  __shared__ double sh[256];
-  for (int v = 0; v < DIAG_VALUES; v++) {
-    double acc = 0;
-    for (long long b = threadIdx.x; b < nblocks; b += blockDim.x) acc += partials[b * DIAG_VALUES + v];
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-      if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[v] = sh[0];
-    __syncthreads();
+// Sums the per-block partials in FP64 in a fixed order (deterministic: the
+// order depends only on the number of step blocks).  Stage 1: block g of
+// FINALIZE_BLOCKS sums a contiguous run of whole partial records with
+// coalesced loads; FINALIZE_THREADS is a multiple of DIAG_VALUES, so thread
+// t always meets value t mod DIAG_VALUES, and the threads of one value are
+// then added in thread order.  Stage 2: one block adds the stage-1 sums in
+// block order.
+__global__ void __launch_bounds__(FINALIZE_THREADS)
+    diag_finalize_blocks_kernel(const double *partials, long long nblocks, double *mid) {
+  __shared__ double sh[FINALIZE_THREADS];
+  const long long per = (nblocks + FINALIZE_BLOCKS - 1) / FINALIZE_BLOCKS;
+  const long long b0 = per * blockIdx.x, b1 = b0 + per < nblocks ? b0 + per : nblocks;
+  const long long end = b1 * DIAG_VALUES;
+  double acc = 0;
+  for (long long k = b0 * DIAG_VALUES + threadIdx.x; k < end; k += FINALIZE_THREADS) acc += partials[k];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < DIAG_VALUES) {
+    double t = 0;
+    for (int k = threadIdx.x; k < FINALIZE_THREADS; k += DIAG_VALUES) t += sh[k];
+    mid[blockIdx.x * DIAG_VALUES + threadIdx.x] = t;
+  }
+}
+__global__ void diag_finalize_kernel(const double *mid, double *out) {
+  if (threadIdx.x < DIAG_VALUES) {
+    double t = 0;
+    for (int g = 0; g < FINALIZE_BLOCKS; g++) t += mid[g * DIAG_VALUES + threadIdx.x];
+    out[threadIdx.x] = t;
   }
 }
 
@@ -656,7 +673,10 @@ extern "C" lbmc_status lbmc_iterate(lbmc_handle *h, int nsteps, unsigned flags) 
     CK(h->ops->step(h->ds, h->step, store, diag, h->stream), "step kernel launch");
     h->step++;
     if (diag) {
-      diag_finalize_kernel<<<1, 256, 0, h->stream>>>(h->ds.partials, h->nblocks, h->diag_out);
+      double *mid = h->ds.partials + DIAG_VALUES * h->nblocks;
+      diag_finalize_blocks_kernel<<<FINALIZE_BLOCKS, FINALIZE_THREADS, 0, h->stream>>>(h->ds.partials,
+                                                                                       h->nblocks, mid);
+      diag_finalize_kernel<<<1, 32, 0, h->stream>>>(mid, h->diag_out);
       CK(cudaGetLastError(), "diagnostic reduction launch");
       h->diag_step = h->step;
     }

@@ -139,6 +139,10 @@ __host__ __device__ constexpr bool moment_conserved(int k) {
 }
 
 constexpr int DIAG_VALUES = 5;  // mass, momentum x/y/z, kinetic energy
+// Two-stage reduction of the per-block diagnostic partials.
+constexpr int FINALIZE_BLOCKS = 256;
+constexpr int FINALIZE_THREADS = 640;  // 20 warps, a multiple of DIAG_VALUES
+static_assert(FINALIZE_THREADS % DIAG_VALUES == 0, "a thread must meet one diagnostic value");
 constexpr int STEP_BLOCK = 256;  // largest block of any step kernel
 // Direct-load kernel: 64-thread blocks and a register cap that keeps 20 of
 // them (40 warps) resident per SM; measured on B200 to beat 128/256-thread
@@ -969,7 +973,7 @@ __device__ __forceinline__ void store_and_reduce(const Node<L, C> &nd, const Ste
 // ------------------------------------------------------------ diagnostics
 
 // Warp-shuffle + shared-memory block reduction of the FP64 sums; one partial
-// per block, summed in a fixed order by diag_finalize_kernel.
+// per block, summed in a fixed order by the finalize kernels (engine.cu).
 template <class C>
 __device__ __forceinline__ void block_diag(const double (&v)[DIAG_VALUES], bool nonfinite,
                                            const StepArgs<C> &a, long long block) {
