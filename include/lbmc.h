@@ -121,7 +121,8 @@ typedef struct lbmc_config {
   int storage;          /* lbmc_storage */
   int streaming;        /* lbmc_streaming */
   unsigned compat;      /* LBMC_COMPAT_* bits */
-  double storage_scale; /* stored value = (f - w) * scale; 0 selects the default */
+  double storage_scale; /* stored value = (f - w) * scale; 0 selects the default (1024 for
+                           FP16, 1 otherwise); FP16 needs a power of two in [2^-15, 2^14] */
   int device;           /* CUDA device ordinal */
   int block_size;       /* reserved for tuning (0) */
   int kernel;           /* lbmc_kernel: 0 auto, 1 direct loads, 2 bulk-copy pipeline */
@@ -247,7 +248,7 @@ typedef struct lbmc_batch_config {
   double force[2];      /* uniform Guo body force */
   int collision_type;   /* LBMC_BGK or LBMC_NTPOR */
   int storage;          /* LBMC_F32, LBMC_F16 or LBMC_BF16 */
-  double storage_scale; /* 0 = default (1024 for FP16) */
+  double storage_scale; /* 0 = default (1024 for FP16); FP16: a power of two in [2^-15, 2^14] */
   int device;
   int block_threads;    /* 0 = autotune (256/512/1024) */
   int steps_per_launch; /* 0 = autotune (check_every or 4*check_every) */

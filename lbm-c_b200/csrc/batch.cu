@@ -526,6 +526,9 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
     return berr(LBMC_ERR_UNSUPPORTED, "batched domains support ColType BGK and NTPOR");
   if (cfg->storage != LBMC_F32 && cfg->storage != LBMC_F16 && cfg->storage != LBMC_BF16)
     return berr(LBMC_ERR_UNSUPPORTED, "batched domains store FP32, FP16 or BF16");
+  if (cfg->storage_scale < 0 || !std::isfinite(cfg->storage_scale) ||
+      (cfg->storage == LBMC_F16 && cfg->storage_scale > 0 && !f16_scale_ok(cfg->storage_scale)))
+    return berr(LBMC_ERR_INVALID_ARG, "storage_scale: >= 0, and for FP16 a power of two in [2^-15, 2^14]");
   if (cudaSetDevice(cfg->device) != cudaSuccess) {
     cudaGetLastError();
     return berr(LBMC_ERR_NO_DEVICE, "no such device");

@@ -196,6 +196,9 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     return fail(LBMC_ERR_INVALID_ARG, "unknown compat bits 0x%x", cfg->compat);
   if (cfg->storage_scale < 0 || !std::isfinite(cfg->storage_scale))
     return fail(LBMC_ERR_INVALID_ARG, "storage_scale must be >= 0");
+  if (cfg->storage == LBMC_F16 && cfg->storage_scale > 0 && !f16_scale_ok(cfg->storage_scale))
+    return fail(LBMC_ERR_INVALID_ARG, "FP16 storage_scale must be a power of two in [2^-15, 2^14] (got %g)",
+                cfg->storage_scale);
   if (cfg->kernel < LBMC_KERNEL_AUTO || cfg->kernel > LBMC_KERNEL_PIPELINED)
     return fail(LBMC_ERR_INVALID_ARG, "unknown kernel choice %d", cfg->kernel);
   if (!dom) return fail(LBMC_ERR_INVALID_ARG, "domain is NULL");

@@ -21,6 +21,7 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 
+#include <cmath>
 #include <type_traits>
 #include <utility>
 
@@ -87,12 +88,32 @@ struct Storage<__nv_bfloat16> {
   static __device__ __forceinline__ void put_any(__nv_bfloat16 *p, C v) { *p = __float2bfloat16_rn(v); }
 };
 
+// FP16 storage scales are powers of two whose inverse is a normal FP16
+// value, so a stored value times the inverse scale is exact in FP32 and
+// the load below can fuse the conversion and the scaling.
+inline bool f16_scale_ok(double scale) {
+  int e = 0;
+  const double m = std::frexp(scale, &e);  // scale = m 2^e, m in [0.5, 1)
+  return m == 0.5 && scale >= 0x1p-15 && scale <= 0x1p14;
+}
+
 // Stored-value conversions with the storage scale applied only where the
-// format uses one.
+// format uses one.  FP16: one mixed-precision FMA, h * (1/scale) + (-0)
+// (the -0 addend keeps every product, signed zeros included, unchanged),
+// equal bit for bit to converting and then multiplying.
 template <class S>
 __device__ __forceinline__ typename Storage<S>::C load_dev(const S *p, typename Storage<S>::C inv_scale) {
-  if constexpr (Storage<S>::SCALED) return Storage<S>::get(p) * inv_scale;
-  else return Storage<S>::get(p);
+  if constexpr (std::is_same<S, __half>::value) {
+    const unsigned short h = __half_as_ushort(*p);
+    const unsigned short s = __half_as_ushort(__float2half_rn(inv_scale));
+    float d;
+    asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(h), "h"(s), "f"(-0.0f));
+    return d;
+  } else if constexpr (Storage<S>::SCALED) {
+    return Storage<S>::get(p) * inv_scale;
+  } else {
+    return Storage<S>::get(p);
+  }
 }
 // Global-memory population store (streaming hint).
 template <class S>

@@ -87,6 +87,20 @@ def test_validate_rejects_bad_parameters(lbmc):
     assert _validate(lbmc, smag_mrt, c_smag=0.1)[0] == lbmc.ERR_UNSUPPORTED
 
 
+def test_validate_fp16_scale_is_a_power_of_two(lbmc):
+    """FP16 stores (f - w) * scale; the load multiplies back by 1/scale in
+    one fused FP16 x FP16 -> FP32 step, exact only for powers of two."""
+    case = make_case("d2q9", (8, 6, 1))
+    for bad in (1000.0, 3.0, 2.0 ** 15, 2.0 ** -16):
+        assert _validate(lbmc, case, storage=lbmc.F16, storage_scale=bad)[0] == lbmc.ERR_INVALID_ARG
+    for ok in (0.0, 1.0, 1024.0, 2048.0, 2.0 ** -15, 2.0 ** 14):
+        assert _validate(lbmc, case, storage=lbmc.F16, storage_scale=ok)[0] == lbmc.OK
+    assert _validate(lbmc, case, storage=lbmc.F32, storage_scale=1000.0)[0] == lbmc.OK
+    with pytest.raises(lbmc.LbmcError) as ei:
+        lbmc.Batch([np.zeros((4, 4))], storage=lbmc.F16, storage_scale=1000.0)
+    assert ei.value.status == lbmc.ERR_INVALID_ARG
+
+
 def test_classify_packs_codes(lbmc):
     case = make_case("d3q15", (6, 5, 4), 3, solids=0.1, partial=0.2, micro="zh")
     st, cfg, dom, keep = _validate(lbmc, case)

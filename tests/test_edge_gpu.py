@@ -61,3 +61,26 @@ def test_zero_steps_is_a_no_op(lbmc):
         eng.iterate(0, lbmc.STORE_MACROS | lbmc.REDUCE_DIAG | lbmc.SYNC)
         assert eng.step() == 0
         np.testing.assert_array_equal(eng.f(), f0)
+
+
+@pytest.mark.parametrize("streaming", ["shift", "aa"])
+def test_fp16_storage_round_trips_every_finite_value(lbmc, streaming):
+    """Every finite FP16 bit pattern h, uploaded as f = w + h / 1024, is
+    stored as exactly h and read back through the load path (one fused
+    FP16 x FP16 -> FP32 FMA) as exactly h / 1024, so lbmc_fetch returns the
+    uploaded f bit for bit (both sides form w + h / 1024 with one double
+    rounding): subnormals and the largest values included, in the shift and
+    the tiled AA layout (Lx = 64)."""
+    bits = np.arange(65536, dtype=np.uint32).astype(np.uint16)
+    bits = bits[(bits & 0x7C00) != 0x7C00]
+    h = bits.view(np.float16).astype(np.float64)
+    case = make_case("d3q15", (64, 67, 1), seed=1)
+    n, q = case.n, case.q
+    w = Restatement(case).equilibrium(np.ones(n), np.zeros((3, n)))[:, :1]
+    dev = np.zeros(q * n)
+    dev[:h.size] = h / 1024.0
+    case.f0 = w + dev.reshape(q, n)
+    sm = lbmc.STREAM_AA if streaming == "aa" else lbmc.STREAM_SHIFT
+    with lbmc.Engine.from_case(case, init_type=lbmc.INIT_F, storage=lbmc.F16, streaming=sm) as eng:
+        got = np.asarray(eng.f()).reshape(q, n)
+    np.testing.assert_array_equal(got, case.f0)
