@@ -32,6 +32,9 @@
 
 using namespace lbmc;
 
+// Values per lbmc_fetch staging chunk (64 MiB of FP64).
+constexpr long long FETCH_CHUNK = 1ll << 23;
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -133,6 +136,8 @@ struct lbmc_handle {
   long long nblocks = 0;
   double *diag_out = nullptr;  // DIAG_VALUES doubles
   long long diag_step = -1;
+  double *fetch_stage = nullptr;  // FP64 staging of lbmc_fetch (allocated on first use)
+  long long fetch_stage_n = 0;
   std::vector<void *> allocations;
 };
 
@@ -699,19 +704,40 @@ extern "C" lbmc_status lbmc_iterate(lbmc_handle *h, int nsteps, unsigned flags) 
   return LBMC_OK;
 }
 
+// dst[k] = (double)src[k] + offset over one chunk of a field.
+template <class C>
+__global__ void widen_kernel(const C *src, double *dst, long long n, double offset) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    dst[k] = (double)src[k] + offset;
+}
+
+// A compute-type field to the caller's FP64 array: the device widens it
+// (and adds the rho offset) into a staging buffer, chunk by chunk, and each
+// chunk goes to the caller's array in one copy, so the host does no
+// conversion pass and allocates no temporary.
 static lbmc_status fetch_compute(lbmc_handle *h, const void *src, double *dst, long long n, double offset) {
-  if (h->ops->csize == 8) {
+  if (h->ops->csize == 8 && offset == 0) {
     CK(cudaMemcpy(dst, src, n * 8, cudaMemcpyDeviceToHost), "fetch field");
-    if (offset != 0)
-      parallel_for(n, [&](long long b, long long e, int) {
-        for (long long k = b; k < e; k++) dst[k] += offset;
-      });
-  } else {
-    std::unique_ptr<float[]> tmp(new float[n]);
-    CK(cudaMemcpy(tmp.get(), src, n * 4, cudaMemcpyDeviceToHost), "fetch field");
-    parallel_for(n, [&](long long b, long long e, int) {
-      for (long long k = b; k < e; k++) dst[k] = (double)tmp[k] + offset;
-    });
+    return LBMC_OK;
+  }
+  const long long chunk = std::min(n, FETCH_CHUNK);
+  if (h->fetch_stage_n < chunk) {
+    double *p = nullptr;
+    CK(cudaMalloc(&p, sizeof(double) * chunk), "fetch staging");
+    h->allocations.push_back(p);
+    h->fetch_stage = p;
+    h->fetch_stage_n = chunk;
+  }
+  for (long long b = 0; b < n; b += chunk) {
+    const long long m = std::min(chunk, n - b);
+    const unsigned grid = (unsigned)std::min<long long>((m + 255) / 256, 4096);
+    if (h->ops->csize == 8)
+      widen_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<const double *>(src) + b, h->fetch_stage, m, offset);
+    else
+      widen_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<const float *>(src) + b, h->fetch_stage, m, offset);
+    CK(cudaGetLastError(), "fetch widen launch");
+    CK(cudaMemcpyAsync(dst + b, h->fetch_stage, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream), "fetch field");
+    CK(cudaStreamSynchronize(h->stream), "fetch field");
   }
   return LBMC_OK;
 }

@@ -231,6 +231,13 @@ def make_domain(n, dim, q, geometry=None, force=None, macro=None, micro=None, u=
     return dom, keep
 
 
+def _checked_out(out, shape):
+    if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.shape == shape
+            and out.flags.c_contiguous):
+        raise ValueError(f"out must be a C-contiguous float64 array of shape {shape}")
+    return out
+
+
 class Engine:
     """One lbmc handle: ``Engine(cfg, domain)`` = lbmc_init."""
 
@@ -268,11 +275,17 @@ class Engine:
         check(library().lbmc_fetch(self.h, field, out.ctypes.data_as(_P), out.nbytes))
         return out
 
-    def rho(self):
-        return self._fetch(FIELD_RHO, np.empty(self.n))
+    def rho(self, out=None):
+        """rho per node (FP64); `out`, if given, is filled and returned."""
+        if out is None:
+            out = np.empty(self.n)
+        return self._fetch(FIELD_RHO, _checked_out(out, (self.n,)))
 
-    def u(self):
-        out = np.empty((self.dim, self.n))
+    def u(self, out=None):
+        """u per node, shape (dim, n) (FP64); `out`, if given, is filled and returned."""
+        if out is None:
+            out = np.empty((self.dim, self.n))
+        _checked_out(out, (self.dim, self.n))
         for d in range(self.dim):
             self._fetch(FIELD_U_X + d, out[d])
         return out

@@ -142,3 +142,14 @@ def test_validate_rejects_sizes(lbmc, length, status):
     dom = lbmc.Domain()
     st = lbmc.library().lbmc_validate(ctypes.byref(cfg), ctypes.byref(dom))
     assert st == getattr(lbmc, status)
+
+
+def test_fetch_out_arrays_are_checked(lbmc):
+    """Engine.rho(out=...) / u(out=...) fill caller arrays of the exact
+    shape and type only (lbmc_fetch writes FP64 node-order arrays)."""
+    from lbmc import _checked_out
+    ok = np.zeros((3, 10))
+    assert _checked_out(ok, (3, 10)) is ok
+    for bad in (np.zeros((3, 10), np.float32), np.zeros((10, 3)), np.zeros((3, 20))[:, ::2], [0.0] * 30):
+        with pytest.raises(ValueError):
+            _checked_out(bad, (3, 10))
