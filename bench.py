@@ -65,7 +65,9 @@ def profiled_traffic(kernel_tag: str):
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+                value = line.split(":", 1)[1].split()[0]
+                # "null": no per-launch DRAM figure (a state that stays in L2)
+                return None if value == "null" else float(value)
     except OSError:
         pass
     return None
@@ -425,11 +427,19 @@ def run_ours(args, world, rank, local):
     eng = workloads.engine_for(lbmc, w, args.storage, device=local, kernel=kernel, streaming=streaming)
     lbmc.check(lbmc.library().lbmc_set_stream(eng.h, stream.cuda_stream))
     mlp = None
-    if args.workload == "closure":
-        # The network's cost does not depend on its weights: a seeded
-        # network with an open input range, so every node evaluates it.
+    if args.workload == "closure" and args.closure_passes > 0:
+        # The network's cost does not depend on its weights: seeded hidden
+        # layers with an open input range, so every node evaluates the
+        # whole network, and an output layer (W3 = 0, b3 = 1) that gives
+        # nu_t = 2e-3 everywhere, so the under-resolved box stays stable
+        # for any number of steps.  (--closure-passes 0: the same box with
+        # Smagorinsky alone.)
         mlp = lbmc.Mlp(seed=1, device=local)
-        mlp.set_normalization(np.zeros(6), np.full(6, 10.0), target_scale=1e-5)
+        params = mlp.params()
+        params[1280:1312] = 0.0  # W3
+        params[1312] = 1.0       # b3
+        mlp.set_params(params)
+        mlp.set_normalization(np.zeros(6), np.full(6, 10.0), target_scale=2e-3)
         mlp.attach(eng, iterations=args.closure_passes)
     # warm-up
     eng.iterate(args.warmup, lbmc.SYNC)

@@ -1083,15 +1083,22 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
         moments(nd);
         collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
       }
-      if constexpr (STREAM == STREAM_AAT_ODD) {
-        // The store addresses equal the load addresses.  Recomputing them
-        // from the three 32-bit x offsets is cheaper than keeping Q 64-bit
-        // pointers live across the collision, which spills 88-116 bytes at
-        // this kernel's register cap (measured: 13% slower with FP16/BF16
-        // storage).  The empty asm hides the equality from the compiler.
+      // The store addresses equal the load addresses.  Recomputing them
+      // from the three 32-bit x offsets is cheaper than keeping Q 64-bit
+      // pointers live across the collision, which spills at this kernel's
+      // register cap: 88-116 bytes in the tiled odd step (13% slower with
+      // FP16/BF16 storage), 20-48 bytes in the shift and plain odd maps.
+      // The 2-byte storages, bound by instruction issue, keep the spill in
+      // the plain maps (the recomputation measured slower there).  The
+      // empty asm hides the equality from the compiler.
+      constexpr bool recompute = STREAM == STREAM_AAT_ODD ||
+                                 ((STREAM == STREAM_AA_ODD || STREAM == STREAM_SHIFT) && sizeof(S) >= 4);
+      if constexpr (recompute) {
         TiledSites tw = ts;
-        asm("" : "+r"(tw.x[0]), "+r"(tw.x[1]), "+r"(tw.x[2]));
-        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, tw, n, ic), out[decltype(ic)::value], scale); });
+        Sites sw = st;
+        if constexpr (STREAM == STREAM_AAT_ODD) asm("" : "+r"(tw.x[0]), "+r"(tw.x[1]), "+r"(tw.x[2]));
+        else asm("" : "+r"(sw.x[0]), "+r"(sw.x[1]), "+r"(sw.x[2]));
+        unroll<Q>([&](auto ic) { store_dev(write_at(f, sw, tw, n, ic), out[decltype(ic)::value], scale); });
       } else {
         unroll<Q>([&](auto ic) { store_dev(write_at(f, st, ts, n, ic), out[decltype(ic)::value], scale); });
       }

@@ -53,3 +53,21 @@ def test_single_rank_aggregation_is_local():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.aggregate_rate(50.0, 2.0, 1) == (25.0, 2.0)
+
+
+def test_every_committed_profile_reads_as_traffic():
+    """bench.py takes the roofline's `traffic` from the summaries under
+    profiles/: every summary that carries the line must parse (a number of
+    bytes per launch, or null where the state stays in L2)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    tags = [f[:-3] for f in os.listdir(os.path.join(ROOT, "profiles")) if f.endswith(".md")]
+    assert tags
+    for tag in tags:
+        with open(os.path.join(ROOT, "profiles", tag + ".md")) as fh:
+            carries = any(line.startswith("traffic_bytes_per_launch:") for line in fh)
+        value = bench.profiled_traffic(tag)
+        if carries and "closure" not in tag:
+            assert isinstance(value, float) and value > 0, tag
+        else:
+            assert value is None or value > 0, tag
