@@ -42,6 +42,7 @@ sys.path.insert(0, ROOT)
 
 UNIT = "GLUPS"
 E2E_STEPS = 500
+REF_ARM_SECONDS = 90.0  # bound of one --impl reference run (warm-up + steps)
 STORAGE_BYTES = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}
 
 
@@ -386,6 +387,15 @@ def run_reference_arm(args, world, rank):
     w = build_workload(args)
     threads = os.cpu_count() or 1
     timer = ReferenceTimer(w, args.ref_nz, threads)
+    # Each step is a bounded sample: a z-crop sized from one timed step so
+    # that warm-up and K steps end within REF_ARM_SECONDS.
+    timer.ref.run(1)  # page-in and thread start
+    t = time.perf_counter()
+    timer.ref.run(1)
+    total = (args.steps + max(1, args.warmup)) * (time.perf_counter() - t)
+    if w.dim == 3 and total > REF_ARM_SECONDS and args.ref_nz > 1:
+        timer.close()
+        timer = ReferenceTimer(w, max(1, int(args.ref_nz * REF_ARM_SECONDS / total)), threads)
     timer.rate(max(1, args.warmup))
     t_total, steps = 0.0, 0
     for _ in range(args.steps):
