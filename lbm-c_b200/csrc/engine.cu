@@ -136,7 +136,7 @@ struct lbmc_handle {
   long long nblocks = 0;
   double *diag_out = nullptr;  // DIAG_VALUES doubles
   long long diag_step = -1;
-  double *fetch_stage = nullptr;  // FP64 staging of lbmc_fetch (allocated on first use)
+  double *fetch_stage = nullptr;  // FP64 staging of uploads and lbmc_fetch (allocated on first use)
   long long fetch_stage_n = 0;
   std::vector<void *> allocations;
 };
@@ -396,23 +396,49 @@ static lbmc_status dev_alloc(lbmc_handle *h, T **p, size_t bytes, const char *wh
   return LBMC_OK;
 }
 
-// Uploads N doubles as the compute type (float or double), converting on
-// the host's cores.
+// dst[k] = (C)(src[k] + offset), or (C)fill everywhere when src is null,
+// over one chunk of a field.
+template <class C>
+__global__ void narrow_kernel(const double *src, C *dst, long long n, double offset, double fill) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    dst[k] = (C)(src ? src[k] + offset : fill);
+}
+
+static lbmc_status ensure_stage(lbmc_handle *h, long long chunk) {
+  if (h->fetch_stage_n >= chunk) return LBMC_OK;
+  double *p = nullptr;
+  CK(cudaMalloc(&p, sizeof(double) * chunk), "staging buffer");
+  h->allocations.push_back(p);
+  h->fetch_stage = p;
+  h->fetch_stage_n = chunk;
+  return LBMC_OK;
+}
+
+// Uploads N doubles as the compute type (float or double): each FP64 chunk
+// of the caller's array goes to the device staging buffer in one copy and
+// the device adds the offset and narrows it, so the host makes no pass over
+// the data and allocates no temporary.
 static lbmc_status upload_compute(lbmc_handle *h, void *dst, const double *src, long long n,
                                   double offset, double fill) {
-  const int cs = h->ops->csize;
-  if (cs == 8) {
-    std::unique_ptr<double[]> tmp(new double[n]);
-    parallel_for(n, [&](long long b, long long e, int) {
-      for (long long k = b; k < e; k++) tmp[k] = src ? src[k] + offset : fill;
-    });
-    CK(cudaMemcpy(dst, tmp.get(), n * 8, cudaMemcpyHostToDevice), "upload field");
-  } else {
-    std::unique_ptr<float[]> tmp(new float[n]);
-    parallel_for(n, [&](long long b, long long e, int) {
-      for (long long k = b; k < e; k++) tmp[k] = (float)(src ? src[k] + offset : fill);
-    });
-    CK(cudaMemcpy(dst, tmp.get(), n * 4, cudaMemcpyHostToDevice), "upload field");
+  const long long chunk = std::min(n, FETCH_CHUNK);
+  if (src) {
+    lbmc_status s = ensure_stage(h, chunk);
+    if (s != LBMC_OK) return s;
+  }
+  for (long long b = 0; b < n; b += chunk) {
+    const long long m = std::min(chunk, n - b);
+    const unsigned grid = (unsigned)std::min<long long>((m + 255) / 256, 4096);
+    if (src)
+      CK(cudaMemcpyAsync(h->fetch_stage, src + b, sizeof(double) * m, cudaMemcpyHostToDevice, h->stream),
+         "upload field");
+    const double *stage = src ? h->fetch_stage : nullptr;
+    if (h->ops->csize == 8)
+      narrow_kernel<double><<<grid, 256, 0, h->stream>>>(stage, static_cast<double *>(dst) + b, m, offset, fill);
+    else
+      narrow_kernel<float><<<grid, 256, 0, h->stream>>>(stage, static_cast<float *>(dst) + b, m, offset, fill);
+    CK(cudaGetLastError(), "upload narrow launch");
+    // The staging buffer is reused by the next chunk.
+    CK(cudaStreamSynchronize(h->stream), "upload field");
   }
   return LBMC_OK;
 }
@@ -721,13 +747,8 @@ static lbmc_status fetch_compute(lbmc_handle *h, const void *src, double *dst, l
     return LBMC_OK;
   }
   const long long chunk = std::min(n, FETCH_CHUNK);
-  if (h->fetch_stage_n < chunk) {
-    double *p = nullptr;
-    CK(cudaMalloc(&p, sizeof(double) * chunk), "fetch staging");
-    h->allocations.push_back(p);
-    h->fetch_stage = p;
-    h->fetch_stage_n = chunk;
-  }
+  lbmc_status s = ensure_stage(h, chunk);
+  if (s != LBMC_OK) return s;
   for (long long b = 0; b < n; b += chunk) {
     const long long m = std::min(chunk, n - b);
     const unsigned grid = (unsigned)std::min<long long>((m + 255) / 256, 4096);
