@@ -209,7 +209,7 @@ def metric_name(args):
 
 
 def run_batch(args, world, rank, local):
-    """Config-5 sweep: independent D2Q9 NTPOR+Guo domains (IMB circles), one
+    """Batched sweep: independent D2Q9 NTPOR+Guo domains (IMB circles), one
     persistent launch replayed from a CUDA graph until every domain's
     max |u(t) - u(t-C)| < tol (C = check interval).  Per-domain latency =
     device time from the run's start to the domain's convergence; the

@@ -204,7 +204,7 @@ def circle_domain(lx, ly, target, rng, rmin=3.0, rmax=12.0, tau=1.0):
 
 
 def batch_sweep(n=4096, lmin=32, lmax=512, seed=5, tau=1.0, square=False):
-    """Config-5 style domains: sides log-uniform in [lmin, lmax] (independent
+    """Batched-sweep domains: sides log-uniform in [lmin, lmax] (independent
     per axis unless square), solid fraction U[0.2, 0.5] of circles radius
     3-12 with IMB edges."""
     rng = np.random.default_rng(seed)

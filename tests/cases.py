@@ -28,7 +28,7 @@ W = {
     "d2q9": np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4),
     "d3q15": np.array([2 / 9] + [1 / 9] * 6 + [1 / 72] * 8),
 }
-# Config-2 style MRT rates: s_e = s_eps = 1.19, s_q = 1.2, s_nu = 1/tau,
+# The porous benchmark's MRT rates: s_e = s_eps = 1.19, s_q = 1.2, s_nu = 1/tau,
 # s_m = 1.2, conserved moments 0.
 def mrt_rates(lattice: str, tau: float):
     if lattice == "d2q9":
@@ -111,7 +111,7 @@ def make_case(lattice: str = "d2q9", length=(16, 12, 1), collision_type: int = 0
     return case
 
 
-def config1_poiseuille() -> Case:
+def poiseuille_channel() -> Case:
     """D2Q9 BGK+Guo Poiseuille channel 128x64, tau 0.8, g_x = 1e-6, walls at
     y = 0 and y = 63 (B = 1), periodic in x, f = w_i (Init 0)."""
     lx, ly = 128, 64

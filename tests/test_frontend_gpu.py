@@ -17,7 +17,7 @@ CLI = os.path.join(ROOT, "lbm-c_b200", "lbmc_run")
 
 
 def channel(tmp_path, lx=128, ly=64, g=1e-6, extra="", **fields):
-    """Config-1 channel: D2Q9 BGK, tau 0.8, Guo force g along x, bounceback
+    """Poiseuille channel: D2Q9 BGK, tau 0.8, Guo force g along x, bounceback
     rows at y = 0 and y = Ly - 1; domain files + input file."""
     dom = tmp_path / "dom"
     dom.mkdir(exist_ok=True)

@@ -2,7 +2,7 @@
 
 Error measure (stated once, used everywhere): for a field X,
     err(X) = max |X_gpu - X_ref| / max |X_ref|
-over all nodes (and components).  North-star bound for FP32 storage: err(rho)
+over all nodes (and components).  Bound for FP32 storage: err(rho)
 and err(u) <= 1e-5 after 1000 steps.  FP64 storage must agree to 1e-10 (the deviation form rounds differently
 from the reference's direct form, so tiny velocities differ by ~1e-17 absolute).
 Reduced-precision storage (f - w in FP16/BF16, FP32 arithmetic) is checked
@@ -14,7 +14,7 @@ import os
 import numpy as np
 import pytest
 
-from cases import config1_poiseuille, make_case, poiseuille_startup
+from cases import make_case, poiseuille_channel, poiseuille_startup
 from oracle.oracle import (COMPAT_AS_IS, COMPAT_MRTPOR_INPLACE, Reference, Restatement,
                            reference_available)
 from test_oracle_pin import GOLDEN, load_golden
@@ -137,10 +137,10 @@ def test_step_counter_continues_across_calls(lbmc, length):
         np.testing.assert_array_equal(a.f(), b.f())
 
 
-def test_config1_poiseuille_parity_1000_steps(lbmc):
-    """North-star gate on the config-1 channel: FP32 engine vs the reference's
+def test_poiseuille_channel_parity_1000_steps(lbmc):
+    """Gate on the D2Q9 Poiseuille channel: FP32 engine vs the reference's
     own FP64 step after 1000 steps, err(rho), err(u) <= 1e-5."""
-    case = config1_poiseuille()
+    case = poiseuille_channel()
     if reference_available("d2q9", "asis"):
         ref = Reference(case, "asis")
     else:
@@ -153,10 +153,10 @@ def test_config1_poiseuille_parity_1000_steps(lbmc):
     assert err(ug, ur) <= 1e-5
 
 
-def test_config1_poiseuille_analytic(lbmc):
-    """Config 1 at t = 2000 against the start-up series, and the steady
+def test_poiseuille_channel_analytic(lbmc):
+    """The channel at t = 2000 against the start-up series, and the steady
     parabola after 2e5 steps (walls half-way between nodes, H = 62)."""
-    case = config1_poiseuille()
+    case = poiseuille_channel()
     with lbmc.Engine.from_case(case) as eng:
         eng.iterate(2000, lbmc.STORE_MACROS | lbmc.SYNC)
         ux = eng.u()[0].reshape(64, 128)
