@@ -410,8 +410,11 @@ def run_reference_arm(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)", "impl": "reference",
-        "config": {"workload": w.name, "nodes": w.n, "sample": timer.sample, "storage": "f64",
-                   "l2": "inputs larger than L2"},
+        "config": {"workload": w.name, "length": list(w.length), "nodes": w.n, "sample": timer.sample,
+                   "storage": "f64", "threads": threads,
+                   # the sampled crop's FP64 populations against the host's caches
+                   "l2": ("sample larger than the host's last-level cache"
+                          if timer.n * w.q * 8 > 64e6 else "sample may fit the host's caches")},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{timer.sample}, {steps} steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -71,3 +71,29 @@ def test_every_committed_profile_reads_as_traffic():
             assert isinstance(value, float) and value > 0, tag
         else:
             assert value is None or value > 0, tag
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` runs LBM-C's own step (host-compiled, all
+    host threads) on a bounded sample of the workload and prints one JSON
+    line with the arm's keys: the same metric and unit as the GPU arm,
+    impl = reference, a cpu_baseline describing the run and an e2e with no
+    host<->device bytes.  Host-only: no GPU is involved."""
+    import json
+    import subprocess
+
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import reference_available
+    if not reference_available("d3q15", "patched"):
+        pytest.skip("oracle/_ref not built")
+    run = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--size", "32", "--steps", "2", "--warmup", "1"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert run.returncode == 0, run.stderr[-2000:]
+    line = json.loads(run.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "GLUPS" and line["value"] > 0
+    assert line["metric"].startswith("GLUPS (D3Q15 MRT porous 32^3")
+    assert line["steps"] == 2 and line["warmup"] == 1 and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["config"]["length"] == [32, 32, 32]
