@@ -1,6 +1,6 @@
 // Step kernels of the engine: one fused kernel per (lattice, storage,
-// collision family, forcing, diagnostics) performs, for every node, the
-// reference's whole time step (LBM-C/solver.cu:10-136):
+// collision family, forcing, diagnostics, streaming layout) performs, for
+// every node, the reference's whole time step (LBM-C/solver.cu:10-136):
 //
 //   load f_i from its in-place shift slot (x - t e_i) mod L  (solver.cu:75-102)
 //   rho, u                                                   (solver.cu:96-108)
@@ -9,6 +9,11 @@
 //   write f_i back to the same slot                          (solver.cu:120-123)
 //   optional rho/u store and FP64 diagnostic partial sums    (solver.cu:126-134,
 //                                                             index.cu:338-373)
+//
+// Besides the reference's shift layout, the same step runs over the AA
+// pattern (one array, even and odd index maps), plain or cut into 64-node
+// tiles (see STREAM_* below); every layout holds the same state after every
+// step, only the places of the values differ.
 //
 // Populations are held as deviations g_i = f_i - w_i in every storage format
 // (FP64, FP32, FP16, BF16; stored value = g_i * scale).  All formulas below are
