@@ -24,8 +24,20 @@ namespace {
 
 int failures = 0;
 
+// Compile-time loop over 0..N-1 on the host (the kernels' unroll is device-only).
+template <int N, class F, int... Is>
+void unroll_host_impl(F &&f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, class F>
+void unroll_host(F &&f) {
+  unroll_host_impl<N>(f, std::make_integer_sequence<int, N>{});
+}
+
 void fail(const char *what, const char *mode, const int *L, long long t, long long n, int i, long long got,
           long long want) {
+  static const int none[3] = {0, 0, 0};
+  if (!L) L = none;
   if (failures++ < 20)
     std::printf("FAIL %s mode=%s L=%dx%dx%d t=%lld node=%lld i=%d got=%lld want=%lld\n", what, mode, L[0], L[1],
                 L[2], t, n, i, got, want);
@@ -151,6 +163,41 @@ void check(int lx, int ly, int lz, bool aa) {
   }
 }
 
+// The tiled odd step adds 32-bit unsigned row and x offsets, which the
+// engine allows only while Q N < 2^32.  At the largest such D3Q15 domain,
+// 1024 x 1024 x 273 (Q N = 4,293,918,720), the offsets of nodes on every
+// face and corner (where the wraps and the largest offsets are) must equal
+// the 64-bit tiled index of the neighbour slot.  No memory is touched.
+template <class L>
+void check_largest_tiled(int lx, int ly, int lz) {
+  const int Q = L::Q;
+  const long long n = (long long)lx * ly * lz;
+  if (Q * n >= (1ll << 32)) {
+    fail("test domain is not tileable", "aat-odd", nullptr, 1, 0, 0, Q * n, 1ll << 32);
+    return;
+  }
+  int L3[3] = {lx, ly, lz}, s[3];
+  for (int k = 0; k < 3; k++) s[k] = 1 % L3[k];  // the odd step's shift
+  const int xs_[] = {0, 1, 63, 64, lx - 65, lx - 64, lx - 1}, ys_[] = {0, 1, ly - 2, ly - 1},
+            zs_[] = {0, 1, lz - 2, lz - 1};
+  for (int z : zs_)
+    for (int y : ys_)
+      for (int x : xs_) {
+        TiledSites ts;
+        ts.init_odd(x / TILE, x % TILE, y, z, s, L3, Q);
+        Sites st;
+        st.init(x, y, z, s, L3);
+        const long long node = x + (long long)lx * (y + (long long)ly * z);
+        unroll_host<Q>([&](auto ic) {
+          constexpr int i = decltype(ic)::value;
+          const unsigned got = ts.row[sel(L::e(1, i))][sel(L::e(2, i))] + ts.x[sel(L::e(0, i))] +
+                               (unsigned)(L::opp(i) * TILE);
+          const long long want = tiled_index(Q, st.template slot<L>(i), L::opp(i));
+          if ((long long)got != want) fail("32-bit offset wraps", "aat-odd", L3, 1, node, i, got, want);
+        });
+      }
+}
+
 }  // namespace
 
 int main() {
@@ -161,6 +208,8 @@ int main() {
     for (auto &s : d3) check<D3Q15>(s[0], s[1], s[2], aa), cases++;
     for (auto &s : d2) check<D2Q9>(s[0], s[1], s[2], aa), cases++;
   }
+  check_largest_tiled<D3Q15>(1024, 1024, 273);
+  cases++;
   if (failures) {
     std::printf("%d failures\n", failures);
     return 1;
