@@ -17,10 +17,17 @@
 # of the needed files from oracle/_ref/gen/, which is deleted after the
 # build; only the .so files stay.  Nothing is copied into the repository.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT
+#    or: LBMC_REFERENCE_ROOT=... oracle/build_ref.sh
+# REFERENCE_ROOT is the directory that holds the reference's LBM-C/ folder.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}/LBM-C"
+ROOT_ARG="${1:-${LBMC_REFERENCE_ROOT:-}}"
+if [ -z "$ROOT_ARG" ]; then
+  echo "build_ref: give the reference root as an argument or in LBMC_REFERENCE_ROOT" >&2
+  exit 2
+fi
+REF="$ROOT_ARG/LBM-C"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/solver.cu" ]; then
   echo "build_ref: reference sources not found at $REF" >&2
