@@ -265,16 +265,19 @@ typedef struct lbmc_batch_domain {
 
 typedef struct lbmc_batch_result {
   long long steps;    /* steps run */
-  double delta_u;     /* last max |u(t) - u(t-1)| measured */
+  double delta_u;     /* last max |u(t) - u(t-1)| measured (NaN once non-finite) */
   double elapsed_ms;  /* device time from the run's start to convergence, -1 if not converged */
   int converged;      /* 1 if delta_u < tol was reached before the step cap */
-  int reserved;
+  int nonfinite;      /* 1 if the domain's velocity became NaN/Inf; it was stopped there */
 } lbmc_batch_result;
 
 lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomains,
                             const lbmc_batch_domain *doms, lbmc_batch **out);
 /* Runs until every domain converged (delta_u < tol, checked every
- * check_every steps) or reached max_steps; results has ndomains entries. */
+ * check_every steps), reached max_steps or became non-finite; results has
+ * ndomains entries.  A domain whose velocity turns NaN/Inf is stopped at the
+ * next check and flagged; the call then returns LBMC_ERR_NAN after filling
+ * results (the reference's NaN exit, LBM-C/index.cu:130-133). */
 lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double tol, int check_every,
                            lbmc_batch_result *results);
 /* LBMC_FIELD_RHO / U_X / U_Y (N doubles; u = j/rho) or LBMC_FIELD_F (9N). */

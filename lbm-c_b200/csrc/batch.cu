@@ -54,8 +54,8 @@ struct BatchDomainDev {
 
 struct BatchStateDev {
   long long t;                  // steps done
-  float delta_u;                // last max |u(t) - u(t-1)|
-  int converged;                // 1 converged, 2 stopped at the step cap
+  float delta_u;                // last max |u(t) - u(t-1)| (NaN once non-finite)
+  int converged;                // 1 converged, 2 stopped at the step cap, 3 stopped non-finite
   unsigned long long done_ns;   // device timer at convergence
 };
 
@@ -120,15 +120,34 @@ __device__ __forceinline__ void batch_node(S *pop, long long pitch, int k, int x
   uy = nd.u[1];
 }
 
+// The convergence measure keeps a non-finite velocity visible: fmaxf
+// returns its non-NaN operand, which would let a diverged domain read as
+// converged, so the maxima below propagate NaN and a non-finite velocity
+// counts as NaN.
+constexpr int STOP_CONVERGED = 1, STOP_CAP = 2, STOP_NONFINITE = 3;
+
+__device__ __forceinline__ float nan_max(float a, float b) { return (b != b || b > a) ? b : a; }
+
+__device__ __forceinline__ float node_delta(float ux, float uy, float2 p) {
+  if (!(isfinite(ux) && isfinite(uy))) return __int_as_float(0x7fffffff);  // positive quiet NaN
+  return fmaxf(fabsf(ux - p.x), fabsf(uy - p.y));
+}
+
+// Convergence test of one domain from its max |u(t) - u(t - C)|.
+__device__ __forceinline__ int stop_code(float m, float tol) {
+  if (m != m) return STOP_NONFINITE;
+  return m < tol ? STOP_CONVERGED : 0;
+}
+
 __device__ __forceinline__ float block_max(float v, float *sh) {
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
+  for (int off = 16; off > 0; off >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, off));
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __syncthreads();
   if (lane == 0) sh[warp] = v;
   __syncthreads();
   float r = 0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = fmaxf(r, sh[w]);
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = nan_max(r, sh[w]);
   return r;
 }
 
@@ -190,10 +209,7 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
         const int c = cls[k];
         float ux, uy;
         batch_node<S, BLEND>(pop, pitch, k, x, y, D.lx, D.ly, sx, sy, c, a, ux, uy);
-        if (test) {
-          const float2 p = up[k];
-          dmax = fmaxf(dmax, fmaxf(fabsf(ux - p.x), fabsf(uy - p.y)));
-        }
+        if (test) dmax = nan_max(dmax, node_delta(ux, uy, up[k]));
         if (save) up[k] = make_float2(ux, uy);
       }
       __syncthreads();
@@ -201,12 +217,12 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
         const float m = block_max(dmax, sh_red);
         if (threadIdx.x == 0) {
           st.delta_u = m;
-          sh_stop = m < A.tol ? 1 : 0;
+          sh_stop = stop_code(m, A.tol);
         }
         __syncthreads();
         stop = sh_stop;
       }
-      if (t + 1 >= A.max_steps) stop = stop ? stop : 2;
+      if (t + 1 >= A.max_steps) stop = stop ? stop : STOP_CAP;
     }
     if (RESIDENT) {
       __syncthreads();
@@ -233,7 +249,8 @@ __global__ void stamp_kernel(unsigned long long *out) { *out = global_ns(); }
 
 // Tail phase: one step of the listed domains, a 256-node tile per block
 // (grid-stride over the tiles).  The convergence test's block maxima go to
-// acc[domain] (non-negative floats compare as their bit patterns).
+// acc[domain] (non-negative floats compare as their bit patterns, and the
+// positive NaN of a non-finite velocity is above every one of them).
 constexpr int WIDE_THREADS = 256;
 struct WideTile {
   int domain, first;
@@ -269,10 +286,7 @@ __global__ void __launch_bounds__(WIDE_THREADS)
       float ux, uy;
       batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, k % D.lx, k / D.lx, D.lx, D.ly, sx, sy,
                            A.cls[D.node_off + k], a, ux, uy);
-      if (test) {
-        const float2 p = up[k];
-        dmax = fmaxf(fabsf(ux - p.x), fabsf(uy - p.y));
-      }
+      if (test) dmax = node_delta(ux, uy, up[k]);
       if (save) up[k] = make_float2(ux, uy);
     }
     if (test) {
@@ -298,10 +312,10 @@ __global__ void batch_wide_finish_kernel(const BatchArgs A, const int *wide, int
     const float m = __int_as_float(acc[d]);
     acc[d] = 0;
     st.delta_u = m;
-    stop = m < A.tol ? 1 : 0;
+    stop = stop_code(m, A.tol);
   }
   t += 1;
-  if (!stop && t >= A.max_steps) stop = 2;
+  if (!stop && t >= A.max_steps) stop = STOP_CAP;
   st.t = t;
   if (stop) {
     st.converged = stop;
@@ -735,12 +749,17 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
     e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(&t0, b->t0, sizeof(t0), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, cudaGetErrorString(e));
+    int nonfinite = 0;
     for (int d = 0; d < b->ndomains; d++) {
       results[d].steps = st[d].t;
       results[d].delta_u = st[d].delta_u;
-      results[d].converged = st[d].converged == 1;
-      results[d].elapsed_ms = st[d].converged ? (double)(st[d].done_ns - t0) * 1e-6 : -1.0;
+      results[d].converged = st[d].converged == STOP_CONVERGED;
+      results[d].nonfinite = st[d].converged == STOP_NONFINITE;
+      results[d].elapsed_ms = st[d].converged == STOP_CONVERGED ? (double)(st[d].done_ns - t0) * 1e-6 : -1.0;
+      nonfinite += results[d].nonfinite;
     }
+    if (nonfinite)
+      return berr(LBMC_ERR_NAN, std::to_string(nonfinite) + " domain(s) became non-finite and were stopped");
   }
   return LBMC_OK;
 }

@@ -49,7 +49,10 @@ lbmc_status fail(lbmc_status s, const char *fmt, ...) {
   return s;
 }
 
+// Reports a CUDA error as the call's status and consumes it, so that a
+// non-sticky error is not left pending for the caller's later CUDA calls.
 lbmc_status cuda_fail(cudaError_t e, const char *what) {
+  cudaGetLastError();
   return fail(e == cudaErrorMemoryAllocation ? LBMC_ERR_ALLOC : LBMC_ERR_CUDA, "%s: %s", what,
               cudaGetErrorString(e));
 }

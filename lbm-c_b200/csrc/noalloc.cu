@@ -28,8 +28,10 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <string>
 
 #include "../../include/lbmc.h"
+#include "engine_internal.h"
 #include "kernels.cuh"
 
 namespace {
@@ -99,15 +101,22 @@ __global__ void __launch_bounds__(NOALLOC_BLOCK)
   }
 }
 
-// Device address of g_partials on the current device (resolved once).
+lbmc_status noalloc_fail(lbmc_status s, const std::string &what) {
+  lbmc::set_last_error("lbmc_macro_sums_noalloc: " + what);
+  return s;
+}
+
+// Device address of g_partials on the current device (resolved once; a
+// cudaDeviceReset by the caller invalidates the cached address, so callers
+// that reset a device must not use this entry point on it afterwards).
 lbmc_status partials_for(int device, double **out) {
-  if (device < 0 || device >= NOALLOC_MAX_DEVICES) return LBMC_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_partials_dev[device]) {
     void *ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, g_partials) != cudaSuccess || !ptr) {
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_partials);
+    if (e != cudaSuccess || !ptr) {
       cudaGetLastError();
-      return LBMC_ERR_CUDA;
+      return noalloc_fail(LBMC_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     }
     g_partials_dev[device] = static_cast<double *>(ptr);
   }
@@ -120,11 +129,23 @@ lbmc_status partials_for(int device, double **out) {
 extern "C" lbmc_status lbmc_macro_sums_noalloc(int device, const double *rho, const double *ux,
                                                const double *uy, const double *uz, long long n,
                                                double *sums, void *cuda_stream) {
-  if (!rho || !ux || !sums || n < 1) return LBMC_ERR_INVALID_ARG;
-  if (n > NOALLOC_MAX_NODES) return LBMC_ERR_INVALID_ARG;  // beyond the fixed scratch
+  if (!rho || !ux || !sums) return noalloc_fail(LBMC_ERR_INVALID_ARG, "rho, ux and sums must not be NULL");
+  if (n < 1) return noalloc_fail(LBMC_ERR_INVALID_ARG, "n must be at least 1");
+  if (n > NOALLOC_MAX_NODES)  // beyond the fixed scratch
+    return noalloc_fail(LBMC_ERR_INVALID_ARG, "n = " + std::to_string(n) + " exceeds the fixed scratch's " +
+                                                  std::to_string(NOALLOC_MAX_NODES) + " nodes");
+  if (device < 0 || device >= NOALLOC_MAX_DEVICES)
+    return noalloc_fail(LBMC_ERR_INVALID_ARG, "device ordinal out of range");
+  // An error left pending by earlier work on this thread would otherwise be
+  // reported after the launches below as if they had failed; it is reported
+  // as what it is and left in place for its owner.
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess)
+    return noalloc_fail(LBMC_ERR_CUDA, std::string("a CUDA error from earlier work is pending (not cleared): ") +
+                                           cudaGetErrorString(pending));
   if (cudaSetDevice(device) != cudaSuccess) {
     cudaGetLastError();
-    return LBMC_ERR_NO_DEVICE;
+    return noalloc_fail(LBMC_ERR_NO_DEVICE, "cudaSetDevice(" + std::to_string(device) + ") failed");
   }
   double *partials = nullptr;
   const lbmc_status st = partials_for(device, &partials);
@@ -132,6 +153,10 @@ extern "C" lbmc_status lbmc_macro_sums_noalloc(int device, const double *rho, co
   const int nblocks = (int)((n + NOALLOC_NODES_PER_BLOCK - 1) / NOALLOC_NODES_PER_BLOCK);
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   noalloc_partials_kernel<<<nblocks, NOALLOC_BLOCK, 0, stream>>>(rho, ux, uy, uz, n, partials);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return noalloc_fail(LBMC_ERR_CUDA, std::string("partials launch: ") + cudaGetErrorString(e));
   noalloc_finalize_kernel<<<1, NOALLOC_BLOCK, 0, stream>>>(partials, nblocks, sums);
-  return cudaGetLastError() == cudaSuccess ? LBMC_OK : LBMC_ERR_CUDA;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return noalloc_fail(LBMC_ERR_CUDA, std::string("finalize launch: ") + cudaGetErrorString(e));
+  return LBMC_OK;
 }

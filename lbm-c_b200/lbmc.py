@@ -342,7 +342,7 @@ class BatchDomain(ctypes.Structure):
 class BatchResult(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_longlong), ("delta_u", ctypes.c_double),
                 ("elapsed_ms", ctypes.c_double), ("converged", ctypes.c_int),
-                ("reserved", ctypes.c_int)]
+                ("nonfinite", ctypes.c_int)]
 
 
 def _batch_lib():
@@ -397,8 +397,15 @@ class Batch:
         self.h, self.n = h, len(geometries)
 
     def run(self, max_steps, tol, check_every=100):
+        """Per-domain results.  A domain that became non-finite raises
+        LbmcError(ERR_NAN) whose ``results`` attribute holds them all."""
         res = (BatchResult * self.n)()
-        check(_batch_lib().lbmc_batch_run(self.h, max_steps, tol, check_every, res))
+        status = _batch_lib().lbmc_batch_run(self.h, max_steps, tol, check_every, res)
+        if status == ERR_NAN:
+            err = LbmcError(status, library().lbmc_last_error().decode())
+            err.results = res
+            raise err
+        check(status)
         return res
 
     def fetch(self, d, field):

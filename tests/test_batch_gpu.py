@@ -92,3 +92,32 @@ def test_batch_tail_phase_is_bit_identical(lbmc, storage, tol, cap):
         assert other[0] == runs[0][0]
         for x, y in zip(runs[0][1], other[1]):
             np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("storage,wide_below", [("f32", -1), ("f32", 100), ("f16", -1)])
+def test_batch_nonfinite_domain_is_reported(lbmc, storage, wide_below):
+    """A domain whose velocity turns non-finite is stopped and flagged, not
+    taken for converged (a max that drops NaN would read it as Delta u = 0).
+    The planted fault is on the host: a negative porosity patch in one
+    domain kept in shared memory and one stepped in HBM, which the
+    Noble-Torczynski blend amplifies until the populations overflow.
+    wide_below = 100 puts the HBM domains in the tail phase from the start."""
+    geoms = [g.copy() for g in domains(seed=9)[:4]]
+    for d in (1, 3):
+        geoms[d][2:6, 2:6] = -50.0
+    with lbmc.Batch(geoms, tau=1.0, force=(1e-6, 0.0), storage=storage,
+                    wide_below=wide_below) as b:
+        if storage == "f32":  # FP16 rows are half as long: all four fit in shared memory
+            assert b.info()["resident_domains"] == 2
+        with pytest.raises(lbmc.LbmcError) as ei:
+            b.run(3000, 1e-12, check_every=50)
+        assert ei.value.status == lbmc.ERR_NAN
+        res = ei.value.results
+        for d in range(4):
+            if d in (1, 3):
+                assert res[d].nonfinite == 1 and res[d].converged == 0
+                assert np.isnan(res[d].delta_u)
+                assert res[d].steps < 3000 and res[d].elapsed_ms == -1.0
+            else:
+                assert res[d].nonfinite == 0 and np.isfinite(res[d].delta_u)
+                assert res[d].steps == 3000

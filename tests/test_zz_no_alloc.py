@@ -61,3 +61,57 @@ def test_noalloc_rejects_sizes_beyond_scratch(lbmc):
                                        x.data_ptr(), None) == lbmc.ERR_INVALID_ARG
     assert lib.lbmc_macro_sums_noalloc(0, x.data_ptr(), x.data_ptr(), None, None, 0,
                                        x.data_ptr(), None) == lbmc.ERR_INVALID_ARG
+
+
+def _check_against_torch(torch, rho, u, s):
+    """FP64 sums of the same device arrays by torch (tolerance relative to
+    the sum of magnitudes, 1e-12)."""
+    terms = [rho, rho * u[0], rho * u[1], rho * u[2], 0.5 * rho * (u * u).sum(0)]
+    for k, t in enumerate(terms):
+        ref = float(t.sum())
+        scale = float(t.abs().sum())
+        assert abs(s[k] - ref) <= 1e-12 * scale, (k, s[k], ref)
+
+
+def _device_fields(torch, n, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    rho = 1 + 0.01 * torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    u = 0.05 * torch.randn((3, n), dtype=torch.float64, device="cuda", generator=g)
+    return rho, u
+
+
+def _call(lbmc, torch, rho, u):
+    out = torch.full((5,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    st = lbmc.library().lbmc_macro_sums_noalloc(0, rho.data_ptr(), u[0].data_ptr(), u[1].data_ptr(),
+                                                 u[2].data_ptr(), rho.numel(), out.data_ptr(), None)
+    assert st == lbmc.OK, lbmc.library().lbmc_last_error()
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def test_noalloc_sums_large_sizes_then_small(lbmc):
+    """More blocks than the finalize kernel's threads (a ragged 5,000,003
+    nodes: 306 blocks), the largest accepted size (2^27 nodes: every slot of
+    the fixed scratch), then a small call that must not read the partials
+    the large calls left behind."""
+    import torch
+    for n, seed in ((5_000_003, 1), (134_217_728, 2), (1000, 3)):
+        rho, u = _device_fields(torch, n, seed)
+        s = _call(lbmc, torch, rho, u)
+        _check_against_torch(torch, rho, u, s)
+        del rho, u
+        torch.cuda.empty_cache()
+
+
+def test_noalloc_reports_its_errors(lbmc):
+    """Rejected calls set a message of their own (not one left over from an
+    earlier call)."""
+    lib = lbmc.library()
+    assert lib.lbmc_macro_sums_noalloc(0, None, None, None, None, 10, None, None) == lbmc.ERR_INVALID_ARG
+    assert b"NULL" in lib.lbmc_last_error()
+    import torch
+    x = torch.zeros(4, dtype=torch.float64, device="cuda")
+    assert lib.lbmc_macro_sums_noalloc(0, x.data_ptr(), x.data_ptr(), None, None, 1 << 28,
+                                       x.data_ptr(), None) == lbmc.ERR_INVALID_ARG
+    assert b"exceeds" in lib.lbmc_last_error()
