@@ -29,12 +29,17 @@ W = {
     "d3q15": np.array([2 / 9] + [1 / 9] * 6 + [1 / 72] * 8),
 }
 # The porous benchmark's MRT rates: s_e = s_eps = 1.19, s_q = 1.2, s_nu = 1/tau,
-# s_m = 1.2, conserved moments 0.
-def mrt_rates(lattice: str, tau: float):
+# s_m = 1.2, conserved moments 0.  With conserved = c the rates on rho and j
+# are c instead, as a TauMRT input line sets them (e.g. "TauMRT 1.0 1.19 1.19
+# 1.0 1.2 1.0 1.2 1.25 1.25"); the reference relaxes every moment with its
+# rate (LBM-C/collision.cu:192-303), so non-zero conserved rates act wherever
+# m_k differs from its equilibrium (with Guo forcing, j - rho u = -F/2).
+def mrt_rates(lattice: str, tau: float, conserved: float = 0.0):
+    c = conserved
     if lattice == "d2q9":
         # rho, e, eps, jx, qx, jy, qy, pxx, pxy
-        return (0.0, 1.19, 1.19, 0.0, 1.2, 0.0, 1.2, 1 / tau, 1 / tau)
-    return (0.0, 1.19, 1.19, 0.0, 1.2, 0.0, 1.2, 0.0, 1.2,
+        return (c, 1.19, 1.19, c, 1.2, c, 1.2, 1 / tau, 1 / tau)
+    return (c, 1.19, 1.19, c, 1.2, c, 1.2, c, 1.2,
             1 / tau, 1 / tau, 1 / tau, 1 / tau, 1 / tau, 1.2)
 
 
@@ -49,11 +54,12 @@ def make_case(lattice: str = "d2q9", length=(16, 12, 1), collision_type: int = 0
               forcing: bool = False, solids: float = 0.0, partial: float = 0.0,
               macro: str | None = None, micro: str | None = None, c_smag: float = 0.0,
               tau: float = 0.8, seed: int = 0, uniform_force: bool = False,
-              u_amp: float = 0.02, compat: int = 0) -> Case:
+              u_amp: float = 0.02, compat: int = 0, mrt_conserved: float = 0.0) -> Case:
     """A random near-equilibrium state with the requested options.
 
     macro: None | "random" (codes 1..15 at ~6% of nodes) | "zh" (rho on faces)
     micro: None | "zh" (Zou-He pressure faces) | "sf" (stress-free faces)
+    mrt_conserved: MRT rate on rho and j (0 = the benchmark's rates)
     """
     _, dim, q = LATTICES[lattice]
     length = tuple(length[:dim]) + (1,) * (3 - dim)
@@ -65,7 +71,7 @@ def make_case(lattice: str = "d2q9", length=(16, 12, 1), collision_type: int = 0
     case = Case(lattice=lattice, length=length, tau=tau, collision_type=collision_type,
                 forcing=forcing, c_smag=c_smag, compat=compat, f0=f0)
     if collision_type >= 2:
-        case.tau_mrt = mrt_rates(lattice, tau)
+        case.tau_mrt = mrt_rates(lattice, tau, mrt_conserved)
     geometry = np.zeros(n)
     if solids > 0:
         geometry[rng.random(n) < solids] = 1.0

@@ -5,7 +5,7 @@ sources by oracle/build_ref.sh) on small seeded problems and stores inputs and
 outputs.  The fixtures let the oracle restatement and the CUDA engine be
 checked against the reference on machines where the reference tree is absent.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [NAME ...]
 
 Each fixture holds: the case parameters, the input arrays, the populations
 after ``nsteps`` steps (natural layout) and the stored rho/u of the last step.
@@ -30,7 +30,8 @@ from oracle.oracle import (COMPAT_AS_IS, COMPAT_MRTPOR_INPLACE, Reference,  # no
 NSTEPS = 7
 SIZES = {"d2q9": (9, 6, 1), "d3q15": (5, 4, 3)}
 
-# name: (lattice, collision_type, forcing, solids, partial, macro, micro, c_smag, variant)
+# name: (lattice, collision_type, forcing, solids, partial, macro, micro, c_smag, variant
+#        [, MRT rate on rho and j])
 CASES = {
     "d2q9_bgk": ("d2q9", 0, False, 0.1, 0.0, None, None, 0.0, "asis"),
     "d2q9_bgk_guo": ("d2q9", 0, True, 0.1, 0.0, None, None, 0.0, "asis"),
@@ -52,20 +53,29 @@ CASES = {
     "d3q15_bgk_zh": ("d3q15", 0, False, 0.0, 0.0, None, "zh", 0.0, "asis"),
     "d3q15_mrt_zh": ("d3q15", 2, False, 0.1, 0.0, None, "zh", 0.0, "patched"),
     "d3q15_smag": ("d3q15", 0, True, 0.1, 0.0, None, None, 0.1, "patched"),
+    # MRT with non-zero rates on the conserved moments (the general MRT kernel)
+    "d2q9_mrt_cons": ("d2q9", 2, False, 0.1, 0.0, None, None, 0.0, "asis", 1.0),
+    "d2q9_mrt_cons_guo": ("d2q9", 2, True, 0.1, 0.0, "random", None, 0.0, "asis", 1.0),
+    "d2q9_mrtpor_cons_guo": ("d2q9", 3, True, 0.1, 0.2, None, None, 0.0, "asis", 1.1),
+    "d3q15_mrt_cons_guo": ("d3q15", 2, True, 0.1, 0.0, "random", None, 0.0, "patched", 1.0),
+    "d3q15_mrtpor_cons_guo": ("d3q15", 3, True, 0.1, 0.2, None, None, 0.0, "patched", 1.1),
+    "d3q15_mrt_cons_zh": ("d3q15", 2, False, 0.1, 0.0, None, "zh", 0.0, "patched", 0.9),
 }
 
 
 def build_case(name: str, seed: int = 11):
-    lat, ct, forcing, solids, partial, macro, micro, smag, variant = CASES[name]
+    lat, ct, forcing, solids, partial, macro, micro, smag, variant, *cons = CASES[name]
     case = make_case(lat, SIZES[lat], ct, forcing, solids=solids, partial=partial,
-                     macro=macro, micro=micro, c_smag=smag, seed=seed)
+                     macro=macro, micro=micro, c_smag=smag, seed=seed,
+                     mrt_conserved=cons[0] if cons else 0.0)
     # The restatement reproduces a reference variant with these compat bits.
     case.compat = COMPAT_AS_IS if variant == "asis" else COMPAT_MRTPOR_INPLACE
     return case, variant
 
 
-def main():
-    for name in CASES:
+def main(names=None):
+    """Writes the named fixtures (default: all)."""
+    for name in names or CASES:
         case, variant = build_case(name)
         if not reference_available(case.lattice, variant):
             raise SystemExit("oracle/_ref is not built: run oracle/build_ref.sh first")
@@ -87,4 +97,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -76,6 +76,30 @@ def test_restatement_matches_reference_live(lat, ct, forcing, bc, smag):
     np.testing.assert_array_equal(b, d)
 
 
+@pytest.mark.parametrize("lat,ct,forcing,bc", [
+    (lat, ct, forcing, bc) for lat in ("d2q9", "d3q15") for ct in (2, 3)
+    for forcing in (False, True) for bc in (None, "random", "zh")])
+def test_restatement_matches_reference_live_conserved_mrt_rates(lat, ct, forcing, bc):
+    """MRT with non-zero rates on rho and j (a TauMRT line that sets them),
+    against the patched reference: the D3Q15 as-is reference relaxes nothing
+    (its M_inv is zero), so only the patched build exercises these rates."""
+    if not reference_available(lat, "patched"):
+        pytest.skip("oracle/_ref not built (needs the reference sources)")
+    length = (13, 6, 1) if lat == "d2q9" else (6, 5, 4)
+    case = make_case(lat, length, ct, forcing, solids=0.12, partial=0.2 if ct == 3 else 0.0,
+                     macro="random" if bc == "random" else None,
+                     micro="zh" if bc == "zh" else None, seed=301 + ct, mrt_conserved=1.05)
+    case.compat = COMPAT_MRTPOR_INPLACE
+    r = Restatement(case)
+    r.run(9)
+    ref = Reference(case, "patched", nthreads=2)
+    ref.run(9)
+    np.testing.assert_array_equal(r.f(), ref.f())
+    (a, b), (c, d) = r.macros(), ref.macros()
+    np.testing.assert_array_equal(a, c)
+    np.testing.assert_array_equal(b, d)
+
+
 @pytest.mark.parametrize("lat", ["d2q9", "d3q15"])
 def test_lattice_invariants(lat):
     case = make_case(lat, (4, 4, 4))

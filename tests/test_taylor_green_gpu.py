@@ -1,0 +1,120 @@
+"""Taylor-Green vortices on the GPU (D3Q15 BGK, the BGK collision of
+LBM-C/collision.cu:49-67, and BGK + Smagorinsky, LBM-C/collision.cu:445-463).
+
+1. Low-Re viscous decay against the analytic solution.  The vortex
+   u = u0 sin(kx) cos(ky), v = -u0 cos(kx) sin(ky), w = 0, uniform in z, is
+   an exact Navier-Stokes solution whose velocity decays as exp(-2 nu k^2 t)
+   (pressure p = -rho u0^2 / 4 (cos 2kx + cos 2ky) balances the advection).
+   On a 64^3 periodic box (one wavelength per 64 nodes), u0 = 0.01, the
+   engine runs FP32 storage from f = f_eq(rho, u).  Checked:
+   - the decay rate of the velocity amplitude between t = 200 and t = 800
+     (after the initial layer) equals 2 nu k^2 within 1e-3 relative;
+   - the amplitude follows exp(-2 nu k^2 t) within 2.5e-3 relative at every
+     sample (this includes the initial-layer offset of starting from f_eq,
+     which the FP64 restatement shows at 0.8e-3 to 0.9e-3 for tau 0.6 / 0.8);
+   - the kinetic energy from the engine's fused FP64 sum equals the host
+     sum of the fetched fields;
+   - the FP32 run equals the FP64 restatement of the same run within 1e-5
+     (err(u) = max|u - u_ref| / max|u_ref|).
+2. The Re = 1600 vortex with Smagorinsky C_s = 0.1 at 64^3: FP32 storage
+   against an FP64-storage engine run of the same problem, kinetic energy and
+   enstrophy (spectral vorticity) over 10 convective times.
+"""
+import numpy as np
+import pytest
+
+import workloads
+from oracle.oracle import Case, Restatement
+
+pytestmark = pytest.mark.gpu
+
+L = 64
+U0 = 0.01
+SAMPLES = (100, 200, 400, 800)
+
+
+def tgv2d_case(tau):
+    n = L * L * L
+    k = 2 * np.pi / L
+    c = np.arange(L) * k
+    z, y, x = np.meshgrid(np.arange(L), c, c, indexing="ij")
+    u = np.zeros((3, n))
+    u[0] = (U0 * np.sin(x) * np.cos(y)).reshape(n)
+    u[1] = (-U0 * np.cos(x) * np.sin(y)).reshape(n)
+    p = -(U0 * U0 / 4) * (np.cos(2 * x) + np.cos(2 * y))
+    rho = 1 + 3 * p.reshape(n)
+    case = Case(lattice="d3q15", length=(L, L, L), tau=tau, collision_type=0, rho=rho, u=u)
+    return case, (tau - 0.5) / 3, k
+
+
+def amplitude(u):
+    return float(np.sqrt(2 * (u[0] ** 2 + u[1] ** 2).mean()))
+
+
+@pytest.mark.parametrize("tau", [0.6, 0.8])
+def test_taylor_green_viscous_decay_analytic(lbmc, tau):
+    case, nu, k = tgv2d_case(tau)
+    ref = Restatement(case)
+    amps, t = {}, 0
+    with lbmc.Engine.from_case(case, init_type=lbmc.INIT_EQUILIBRIUM) as eng:
+        for T in SAMPLES:
+            eng.iterate(T - t, lbmc.STORE_MACROS | lbmc.REDUCE_DIAG | lbmc.SYNC)
+            t = T
+            rho, u = eng.rho(), eng.u()
+            d = eng.diag()
+            ke = 0.5 * (rho * (u * u).sum(0)).sum()
+            assert abs(d.kinetic_energy - ke) <= 1e-12 * ke
+            amps[T] = amplitude(u)
+            exact = np.exp(-2 * nu * k * k * T)
+            rel = amps[T] / U0 / exact - 1
+            print(f"tau {tau} t {T}: amplitude / analytic - 1 = {rel:.2e}")
+            assert abs(rel) <= 2.5e-3
+        u_gpu = u
+    rate = -np.log(amps[800] / amps[200]) / 600
+    print(f"tau {tau}: decay rate / (2 nu k^2) - 1 = {rate / (2 * nu * k * k) - 1:.2e}")
+    assert abs(rate / (2 * nu * k * k) - 1) <= 1e-3
+    # the same run in FP64 on the CPU
+    case.f0 = ref.equilibrium(case.rho, case.u)
+    ref = Restatement(case)
+    ref.run(800)
+    _, u_ref = ref.macros()
+    assert np.abs(u_gpu - u_ref).max() / np.abs(u_ref).max() <= 1e-5
+
+
+def enstrophy(u, n):
+    """0.5 <|curl u|^2> with spectral derivatives on the periodic cube."""
+    f = [np.fft.fftn(u[c].reshape(n, n, n)) for c in range(3)]  # axes (z, y, x)
+    kk = 2 * np.pi * np.fft.fftfreq(n)
+    kz, ky, kx = np.meshgrid(kk, kk, kk, indexing="ij")
+    d = lambda comp, kv: np.real(np.fft.ifftn(1j * kv * f[comp]))  # noqa: E731
+    wx = d(2, ky) - d(1, kz)
+    wy = d(0, kz) - d(2, kx)
+    wz = d(1, kx) - d(0, ky)
+    return 0.5 * float((wx * wx + wy * wy + wz * wz).mean())
+
+
+def test_taylor_green_smagorinsky_fp32_vs_fp64(lbmc):
+    """Re 1600, u0 0.05, C_s 0.1 at 64^3 for 10 convective times
+    (T_c = L / (2 pi u0)); FP32 storage against FP64 storage of the same
+    engine.  Bounds: kinetic energy 1e-4 and enstrophy 1e-3 relative to their
+    FP64 values at every sample."""
+    w = workloads.taylor_green(L=L, u0=0.05, re=1600.0, c_smag=0.1)
+    tc = w.params["ell"] / w.params["u0"]
+    samples = [int(round(m * tc)) for m in (1, 2, 4, 6, 8, 10)]
+    series = {}
+    for storage in ("f64", "f32"):
+        out, t = [], 0
+        with workloads.engine_for(lbmc, w, storage, streaming=lbmc.STREAM_AA) as eng:
+            for T in samples:
+                eng.iterate(T - t, lbmc.STORE_MACROS | lbmc.REDUCE_DIAG | lbmc.SYNC)
+                t = T
+                out.append((eng.diag().kinetic_energy, enstrophy(eng.u(), L)))
+        series[storage] = np.array(out)
+    ke64, en64 = series["f64"].T
+    ke32, en32 = series["f32"].T
+    eke = np.abs(ke32 - ke64) / ke64
+    een = np.abs(en32 - en64) / en64
+    print("KE(t)/KE(0):", np.round(ke64 / ke64[0], 4), "KE err:", eke, "enstrophy err:", een)
+    assert ke64[-1] < 0.9 * ke64[0]  # the vortex decays
+    assert eke.max() <= 1e-4
+    assert een.max() <= 1e-3
