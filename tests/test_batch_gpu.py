@@ -119,5 +119,6 @@ def test_batch_nonfinite_domain_is_reported(lbmc, storage, wide_below):
                 assert np.isnan(res[d].delta_u)
                 assert res[d].steps < 3000 and res[d].elapsed_ms == -1.0
             else:
+                # small FP32 domains may reach an exact fixed point (delta_u = 0)
                 assert res[d].nonfinite == 0 and np.isfinite(res[d].delta_u)
-                assert res[d].steps == 3000
+                assert res[d].converged == 1 or res[d].steps == 3000
