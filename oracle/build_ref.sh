@@ -6,6 +6,8 @@
 #   oracle/_ref/libref_d2q9_asis.so     D2Q9, reference as is
 #   oracle/_ref/libref_d2q9_patched.so  D2Q9, Smagorinsky q_bar zero-initialised
 #   oracle/_ref/libref_d3q15_asis.so    D3Q15, reference as is
+#   oracle/_ref/libref_reader_{d2q9,d3q15}.so  the input-file reader
+#       (infile_reader.cu) for each lattice, unpatched
 #   oracle/_ref/libref_d3q15_patched.so D3Q15 with the documented fixes:
 #       macros.cu:97-115  M_inv integer divisions -> floating point
 #       collision.cu:492-496  (-7/3) -> (-7.0/3.0)
@@ -42,7 +44,7 @@ build_variant() {
   local gen="$OUT/gen/${lat}_${variant}"
   rm -rf "$gen"
   mkdir -p "$gen/boundary_conditions/d2q9" "$gen/boundary_conditions/d3q15"
-  for f in macros.cu data_types.cuh solver.cu solver.cuh collision.cu collision.cuh; do
+  for f in macros.cu data_types.cuh solver.cu solver.cuh collision.cu collision.cuh infile_reader.cu; do
     cp "$REF/$f" "$gen/$f"
   done
   for f in macro_bc.cu macro_bc.cuh micro_bc.cuh \
@@ -64,6 +66,12 @@ build_variant() {
   fi
   $CXX $FLAGS -I "$gen" -I "$HERE/shim_include" "$HERE/ref_shim.cpp" \
       -o "$OUT/libref_${lat}_${variant}.so"
+  if [ "$variant" = "asis" ]; then
+    # The input-file reader (infile_reader.cu), unpatched.
+    $CXX $FLAGS -I "$gen" -I "$HERE/shim_include" "$HERE/ref_reader_shim.cpp" \
+        -o "$OUT/libref_reader_${lat}.so"
+    echo "built $OUT/libref_reader_${lat}.so"
+  fi
   rm -rf "$gen"
   echo "built $OUT/libref_${lat}_${variant}.so"
 }
