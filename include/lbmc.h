@@ -65,12 +65,19 @@ typedef enum lbmc_status {
 typedef enum lbmc_lattice { LBMC_D2Q9 = 0, LBMC_D3Q15 = 1 } lbmc_lattice;
 
 /* Population storage in HBM.  All formats hold f_i - w_i (deviation from the
- * rest-state weight); arithmetic is FP32, or FP64 for LBMC_F64. */
+ * rest-state weight); arithmetic is FP32, or FP64 for LBMC_F64.
+ * LBMC_F16_SR is LBMC_F16 (same format and scale) whose step results are
+ * written with stochastic rounding: each value rounds up with probability
+ * equal to its distance from the FP16 value below it, from random bits that
+ * depend only on (node, step, population), so runs are reproducible and
+ * every streaming layout gives the same bits.  The initial upload rounds to
+ * nearest.  Not available to the batched domains (lbmc_batch_*). */
 typedef enum lbmc_storage {
   LBMC_F32 = 0,
   LBMC_F16 = 1,
   LBMC_BF16 = 2,
-  LBMC_F64 = 3
+  LBMC_F64 = 3,
+  LBMC_F16_SR = 4
 } lbmc_storage;
 
 /* ColType codes of LBM-C/infile_reader.cu:118-144. */
@@ -122,7 +129,8 @@ typedef struct lbmc_config {
   int streaming;        /* lbmc_streaming */
   unsigned compat;      /* LBMC_COMPAT_* bits */
   double storage_scale; /* stored value = (f - w) * scale; 0 selects the default (1024 for
-                           FP16, 1 otherwise); FP16 needs a power of two in [2^-15, 2^14] */
+                           FP16 and FP16_SR, 1 otherwise); FP16 and FP16_SR need a power of
+                           two in [2^-15, 2^14] */
   int device;           /* CUDA device ordinal */
   int block_size;       /* reserved for tuning (0) */
   int kernel;           /* lbmc_kernel: 0 auto, 1 direct loads, 2 bulk-copy pipeline */

@@ -80,6 +80,7 @@ const LatticeStorageOps *select_ops(int lattice, int storage) {
       case LBMC_F16: return ops_d2q9_f16();
       case LBMC_BF16: return ops_d2q9_bf16();
       case LBMC_F64: return ops_d2q9_f64();
+      case LBMC_F16_SR: return ops_d2q9_f16sr();
     }
   } else {
     switch (storage) {
@@ -87,6 +88,7 @@ const LatticeStorageOps *select_ops(int lattice, int storage) {
       case LBMC_F16: return ops_d3q15_f16();
       case LBMC_BF16: return ops_d3q15_bf16();
       case LBMC_F64: return ops_d3q15_f64();
+      case LBMC_F16_SR: return ops_d3q15_f16sr();
     }
   }
   return nullptr;
@@ -165,7 +167,9 @@ extern "C" lbmc_status lbmc_config_default(lbmc_config *cfg, int lattice) {
   return LBMC_OK;
 }
 
-static double default_scale(int storage) { return storage == LBMC_F16 ? 1024.0 : 1.0; }
+static double default_scale(int storage) {
+  return storage == LBMC_F16 || storage == LBMC_F16_SR ? 1024.0 : 1.0;
+}
 
 // Checks a configuration and domain without touching the GPU.
 extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *dom) {
@@ -192,7 +196,7 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     return fail(LBMC_ERR_UNSUPPORTED, "Smagorinsky is only defined for the BGK family (ColType BGK/NTPOR)");
   if (!(cfg->c_smag >= 0.0) || !std::isfinite(cfg->c_smag))
     return fail(LBMC_ERR_INVALID_ARG, "c_smag must be >= 0 (got %g)", cfg->c_smag);
-  if (cfg->storage < LBMC_F32 || cfg->storage > LBMC_F64)
+  if (cfg->storage < LBMC_F32 || cfg->storage > LBMC_F16_SR)
     return fail(LBMC_ERR_INVALID_ARG, "unknown storage %d", cfg->storage);
   if (cfg->streaming != LBMC_STREAM_SHIFT && cfg->streaming != LBMC_STREAM_AA)
     return fail(LBMC_ERR_INVALID_ARG, "unknown streaming scheme %d", cfg->streaming);
@@ -204,7 +208,8 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     return fail(LBMC_ERR_INVALID_ARG, "unknown compat bits 0x%x", cfg->compat);
   if (cfg->storage_scale < 0 || !std::isfinite(cfg->storage_scale))
     return fail(LBMC_ERR_INVALID_ARG, "storage_scale must be >= 0");
-  if (cfg->storage == LBMC_F16 && cfg->storage_scale > 0 && !f16_scale_ok(cfg->storage_scale))
+  if ((cfg->storage == LBMC_F16 || cfg->storage == LBMC_F16_SR) && cfg->storage_scale > 0 &&
+      !f16_scale_ok(cfg->storage_scale))
     return fail(LBMC_ERR_INVALID_ARG, "FP16 storage_scale must be a power of two in [2^-15, 2^14] (got %g)",
                 cfg->storage_scale);
   if (cfg->kernel < LBMC_KERNEL_AUTO || cfg->kernel > LBMC_KERNEL_PIPELINED)

@@ -79,5 +79,7 @@ const LatticeStorageOps *ops_d3q15_f32();
 const LatticeStorageOps *ops_d3q15_f16();
 const LatticeStorageOps *ops_d3q15_bf16();
 const LatticeStorageOps *ops_d3q15_f64();
+const LatticeStorageOps *ops_d2q9_f16sr();
+const LatticeStorageOps *ops_d3q15_f16sr();
 
 }  // namespace lbmc

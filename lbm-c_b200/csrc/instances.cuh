@@ -48,6 +48,7 @@ struct Launchers {
     a.table = d.table_dev;
     a.closure = static_cast<const MlpStep *>(d.closure);
     a.mlp = d.closure_consts;
+    a.sr_seed = sr_step_seed(t);
     return a;
   }
 

@@ -84,6 +84,32 @@ struct Storage<__half> {
   static __device__ __forceinline__ void put(__half *p, C v) { __stcs(p, __float2half_rn(v)); }
   static __device__ __forceinline__ void put_any(__half *p, C v) { *p = __float2half_rn(v); }
 };
+// FP16 written with stochastic rounding (LBMC_F16_SR): the same 2-byte
+// format and scale as __half, so loads are identical; the step kernels write
+// their results through store_node_sr below, which rounds each value up
+// with probability equal to its distance from the FP16 value below it
+// (relative to the FP16 spacing there), so the rounding error has zero
+// mean.  Round-to-nearest FP16 storage loses the slow flow's velocity
+// signal to a rounding bias that accumulates step after step; stochastic
+// rounding turns it into noise that averages out.  Single stores (initial
+// upload, shared-memory copies) round to nearest.
+struct __align__(2) half_sr {
+  unsigned short bits;
+};
+template <>
+struct Storage<half_sr> {
+  using C = float;
+  static constexpr bool SCALED = true;
+  static __device__ __forceinline__ C get(const half_sr *p) { return __half2float(__ushort_as_half(p->bits)); }
+  static __device__ __forceinline__ void put(half_sr *p, C v) {
+    __stcs(reinterpret_cast<unsigned short *>(p), __half_as_ushort(__float2half_rn(v)));
+  }
+  static __device__ __forceinline__ void put_any(half_sr *p, C v) { p->bits = __half_as_ushort(__float2half_rn(v)); }
+};
+template <class S>
+__host__ __device__ constexpr bool stochastic_storage() {
+  return std::is_same<S, half_sr>::value;
+}
 template <>
 struct Storage<__nv_bfloat16> {
   using C = float;
@@ -108,8 +134,8 @@ inline bool f16_scale_ok(double scale) {
 // equal bit for bit to converting and then multiplying.
 template <class S>
 __device__ __forceinline__ typename Storage<S>::C load_dev(const S *p, typename Storage<S>::C inv_scale) {
-  if constexpr (std::is_same<S, __half>::value) {
-    const unsigned short h = __half_as_ushort(*p);
+  if constexpr (std::is_same<S, __half>::value || std::is_same<S, half_sr>::value) {
+    const unsigned short h = *reinterpret_cast<const unsigned short *>(p);
     const unsigned short s = __half_as_ushort(__float2half_rn(inv_scale));
     float d;
     asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(h), "h"(s), "f"(-0.0f));
@@ -131,6 +157,66 @@ template <class S>
 __device__ __forceinline__ void store_smem(S *p, typename Storage<S>::C v, typename Storage<S>::C scale) {
   if constexpr (Storage<S>::SCALED) Storage<S>::put_any(p, v * scale);
   else Storage<S>::put_any(p, v);
+}
+
+// ------------------------------------------------ stochastic rounding bits
+
+// 32-bit integer finaliser (xor-shift and multiply rounds with the
+// "lowbias32" constants of C. Wellons' hash-prospector search): every input
+// bit affects every output bit.
+__host__ __device__ __forceinline__ unsigned mix32(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+// Per-step seed of the stochastic rounding (the step counter t, 64-bit).
+__host__ __device__ __forceinline__ unsigned sr_step_seed(long long t) {
+  return mix32((unsigned)t ^ mix32((unsigned)((unsigned long long)t >> 32) + 0x9e3779b9u));
+}
+// Odd multipliers that turn one hashed word into further random words: the
+// upper half of the 64-bit product h * m_k depends on every bit of h.
+__host__ __device__ constexpr unsigned sr_multiplier(int k) {
+  return k == 1 ? 0x9e3779b1u : k == 2 ? 0x85ebca77u : k == 3 ? 0xc2b2ae3du : k == 4 ? 0x27d4eb2fu
+       : k == 5 ? 0x165667b1u : k == 6 ? 0xd3a2646du : 0xfd7046c5u;
+}
+
+// cvt.rs.f16x2.f32: hi goes to the upper, lo to the lower half of the
+// result; the low 13 bits of each 16-bit half of rbits are the random bits
+// that round the value of that half (measured on the B200: a value rounds
+// up when those bits plus its 13 dropped mantissa bits reach 2^13).
+__device__ __forceinline__ unsigned cvt_rs_f16x2(float hi, float lo, unsigned rbits) {
+  unsigned d;
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+  return d;
+}
+
+// Writes a node's Q post-collision values with stochastic rounding, two per
+// conversion: population pair (2k, 2k+1) takes random word k, word 0 being
+// mix32(node ^ step seed) and word k > 0 its product with sr_multiplier(k).
+// The bits depend only on (node, step, population), so every streaming
+// layout writes the same values.  ptr(ic) is the destination of population
+// ic; GLOBAL selects the streaming-hint global store (else a plain store,
+// for shared memory).
+template <int Q, bool GLOBAL, class Ptr>
+__device__ __forceinline__ void store_node_sr(const float (&out)[Q], float scale, unsigned key, Ptr &&ptr) {
+  const unsigned h = mix32(key);
+  auto put16 = [](half_sr *p, unsigned short v) {
+    if constexpr (GLOBAL) __stcs(reinterpret_cast<unsigned short *>(p), v);
+    else p->bits = v;
+  };
+  unroll<(Q + 1) / 2>([&](auto pc) {
+    constexpr int k = decltype(pc)::value;
+    constexpr int i0 = 2 * k, i1 = 2 * k + 1;
+    const unsigned r = k == 0 ? h : __umulhi(h, sr_multiplier(k));
+    float hi = 0.0f;
+    if constexpr (i1 < Q) hi = out[i1] * scale;
+    const unsigned d = cvt_rs_f16x2(hi, out[i0] * scale, r);
+    put16(ptr(std::integral_constant<int, i0>{}), (unsigned short)(d & 0xffffu));
+    if constexpr (i1 < Q) put16(ptr(std::integral_constant<int, i1>{}), (unsigned short)(d >> 16));
+  });
 }
 
 // ------------------------------------------------------------ node classes
@@ -210,6 +296,7 @@ struct StepArgs {
   const uint16_t *table;        // 256 class-table entries (device memory)
   const MlpStep *closure;       // learned closure (COL_BGK_MLP): weights
   MlpConsts mlp;                // and its scalars
+  unsigned sr_seed;             // stochastic-rounding seed of this step (sr_step_seed(t))
 };
 
 constexpr unsigned ERROR_TIMEOUT = 1u;
@@ -1098,14 +1185,21 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
       // empty asm hides the equality from the compiler.
       constexpr bool recompute = STREAM == STREAM_AAT_ODD ||
                                  ((STREAM == STREAM_AA_ODD || STREAM == STREAM_SHIFT) && sizeof(S) >= 4);
+      auto store_all = [&](const Sites &sw, const TiledSites &tw) {
+        if constexpr (stochastic_storage<S>())
+          store_node_sr<Q, true>(out, scale, (unsigned)n ^ a.sr_seed,
+                                 [&](auto ic) { return write_at(f, sw, tw, n, ic); });
+        else
+          unroll<Q>([&](auto ic) { store_dev(write_at(f, sw, tw, n, ic), out[decltype(ic)::value], scale); });
+      };
       if constexpr (recompute) {
         TiledSites tw = ts;
         Sites sw = st;
         if constexpr (STREAM == STREAM_AAT_ODD) asm("" : "+r"(tw.x[0]), "+r"(tw.x[1]), "+r"(tw.x[2]));
         else asm("" : "+r"(sw.x[0]), "+r"(sw.x[1]), "+r"(sw.x[2]));
-        unroll<Q>([&](auto ic) { store_dev(write_at(f, sw, tw, n, ic), out[decltype(ic)::value], scale); });
+        store_all(sw, tw);
       } else {
-        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, ts, n, ic), out[decltype(ic)::value], scale); });
+        store_all(st, ts);
       }
       store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
     }
@@ -1142,7 +1236,11 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
       collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, fluid && cls ? a.table[cls] : 0u, out, fluid);
       if (!fluid) collide_solid(nd, out);
       if (active) {
-        unroll<Q>([&](auto ic) { store_dev(write_at(f, st, ts, n, ic), out[decltype(ic)::value], scale); });
+        if constexpr (stochastic_storage<S>())
+          store_node_sr<Q, true>(out, scale, (unsigned)n ^ a.sr_seed,
+                                 [&](auto ic) { return write_at(f, st, ts, n, ic); });
+        else
+          unroll<Q>([&](auto ic) { store_dev(write_at(f, st, ts, n, ic), out[decltype(ic)::value], scale); });
         store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
       }
     }
@@ -1382,12 +1480,16 @@ __global__ void __launch_bounds__(STEP_BLOCK + 32)
           moments(nd);
           collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, cls ? a.table[cls] : 0u, out);
         }
-        unroll<Q>([&](auto ic) {
+        auto slot_of = [&](auto ic) {
           constexpr int i = decltype(ic)::value;
           constexpr int ex = L::e(0, i);
           const int xs = ex > 0 ? xp : (ex < 0 ? xm : x);
-          store_smem(sb + i * lx + xs, out[i], scale);
-        });
+          return sb + i * lx + xs;
+        };
+        if constexpr (stochastic_storage<S>())
+          store_node_sr<Q, false>(out, scale, (unsigned)n ^ a.sr_seed, slot_of);
+        else
+          unroll<Q>([&](auto ic) { store_smem(slot_of(ic), out[decltype(ic)::value], scale); });
         store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
       }
       fence_proxy_async();

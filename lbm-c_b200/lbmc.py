@@ -22,7 +22,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "lbmc.h")
 OK, ERR_INVALID_ARG, ERR_UNSUPPORTED, ERR_CUDA, ERR_ALLOC, ERR_NAN, ERR_TIMEOUT, ERR_IO, \
     ERR_BUFFER_SIZE, ERR_NO_DEVICE = range(10)
 D2Q9, D3Q15 = 0, 1
-F32, F16, BF16, F64 = 0, 1, 2, 3
+F32, F16, BF16, F64, F16_SR = 0, 1, 2, 3, 4
 BGK, NTPOR, MRT, MRTPOR = 0, 1, 2, 3
 INIT_STATIC, INIT_EQUILIBRIUM, INIT_F = 0, 1, 2
 STREAM_SHIFT, STREAM_AA = 0, 1
@@ -36,7 +36,7 @@ STORE_MACROS, REDUCE_DIAG, SYNC = 1, 2, 4
 FIELD_RHO, FIELD_U_X, FIELD_U_Y, FIELD_U_Z, FIELD_F, FIELD_DIAG = range(6)
 
 LATTICE_IDS = {"d2q9": D2Q9, "d3q15": D3Q15}
-STORAGE_IDS = {"f32": F32, "f16": F16, "bf16": BF16, "f64": F64}
+STORAGE_IDS = {"f32": F32, "f16": F16, "bf16": BF16, "f64": F64, "f16sr": F16_SR}
 
 _P = ctypes.c_void_p
 _DP = ctypes.POINTER(ctypes.c_double)

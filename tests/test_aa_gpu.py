@@ -9,7 +9,8 @@ must be bit-identical: populations (natural order, un-mapped by
 lbmc_fetch), stored rho/u and the FP64 diagnostic sums, after odd and
 even step counts, for every collision type, forcing, macro, Zou-He and
 stress-free boundaries, partial solids, both lattices, FP64/FP32/FP16
-storage, and the learned closure in FP64 (its FP32 kernels agree to the
+storage (FP16 also with stochastic rounding, whose random bits depend on
+node, step and population only), and the learned closure in FP64 (its FP32 kernels agree to the
 FP32 rounding level).  The shift layout is itself checked
 against the oracle (test_parity_gpu.py), which pins AA to it as well.
 """
@@ -43,7 +44,7 @@ LENGTHS = {("d2q9", False): (37, 21, 1), ("d3q15", False): (19, 11, 9),
 
 
 @pytest.mark.parametrize("tiled", [False, True], ids=["plain", "tiled"])
-@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f16sr", "f64"])
 @pytest.mark.parametrize("lat,ct,forcing,bc,smag", AA_COMBOS)
 def test_aa_equals_shift(lbmc, lat, ct, forcing, bc, smag, storage, tiled):
     if storage != "f32" and (forcing or smag or ct in (1, 2)):

@@ -64,7 +64,8 @@ def test_zero_steps_is_a_no_op(lbmc):
 
 
 @pytest.mark.parametrize("streaming", ["shift", "aa"])
-def test_fp16_storage_round_trips_every_finite_value(lbmc, streaming):
+@pytest.mark.parametrize("storage", ["f16", "f16sr"])
+def test_fp16_storage_round_trips_every_finite_value(lbmc, streaming, storage):
     """Every finite FP16 bit pattern h, uploaded as f = w + h / 1024, is
     stored as exactly h and read back through the load path (one fused
     FP16 x FP16 -> FP32 FMA) as exactly h / 1024, so lbmc_fetch returns the
@@ -81,6 +82,7 @@ def test_fp16_storage_round_trips_every_finite_value(lbmc, streaming):
     dev[:h.size] = h / 1024.0
     case.f0 = w + dev.reshape(q, n)
     sm = lbmc.STREAM_AA if streaming == "aa" else lbmc.STREAM_SHIFT
-    with lbmc.Engine.from_case(case, init_type=lbmc.INIT_F, storage=lbmc.F16, streaming=sm) as eng:
+    with lbmc.Engine.from_case(case, init_type=lbmc.INIT_F, storage=lbmc.STORAGE_IDS[storage],
+                               streaming=sm) as eng:
         got = np.asarray(eng.f()).reshape(q, n)
     np.testing.assert_array_equal(got, case.f0)

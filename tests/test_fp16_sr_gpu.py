@@ -1,0 +1,90 @@
+"""FP16 (f - w) storage written with stochastic rounding (LBMC_F16_SR).
+
+1. The rounding itself: a uniform periodic state under a uniform Guo force
+   gives every node the same FP32 post-collision values after one step, so
+   the stored FP16 values of a population are the two FP16 neighbours lo <
+   v < hi of that value, and the fraction of nodes that rounded up must be
+   (v - lo) / (hi - lo) within 5 standard deviations of a binomial count
+   (v from the FP64 restatement; its difference from the FP32 value is
+   ~1e-4 of the FP16 spacing).  The decisions one node makes for the
+   populations paired in one conversion, and for populations of different
+   pairs, are independent (|correlation| < 0.02 over 2^18 nodes).
+2. Accuracy, the purpose of the format: the porous-medium MRT flow (the
+   benchmark's sphere pack, Zou-He pressure faces, its relaxation rates) on
+   128 x 64 x 32 nodes for 2000 steps against an FP64-storage run of the
+   same engine.  Bound: L2 relative velocity error <= 1e-3 (the accuracy
+   target for 2-byte storage); round-to-nearest FP16 is measured beside it
+   and must be worse.
+"""
+import numpy as np
+import pytest
+
+import workloads
+from cases import make_case
+from oracle.oracle import Restatement
+
+pytestmark = pytest.mark.gpu
+
+
+def test_stochastic_rounding_is_unbiased(lbmc):
+    case = make_case("d3q15", (64, 64, 64), 0, True, seed=2)
+    n, q = case.n, case.q
+    w = np.array([2 / 9] + [1 / 9] * 6 + [1 / 72] * 8)
+    rho0, u0 = 1.0 + 3.1e-4, np.array([1.7e-3, -0.9e-3, 0.4e-3])
+    r = Restatement(case)
+    case.f0 = np.repeat(r.equilibrium(np.full(1, rho0), u0[:, None]), n, axis=1)
+    case.force = np.tile(np.array([2.3e-5, 1.1e-5, -0.7e-5])[:, None], (1, n))
+    case.geometry = np.zeros(n)
+    r = Restatement(case)
+    r.run(1)
+    exact = (r.f()[:, 0] - w) * 1024.0  # the scaled value every node rounds
+    with lbmc.Engine.from_case(case, storage=lbmc.F16_SR, streaming=lbmc.STREAM_AA) as eng:
+        eng.iterate(1, lbmc.SYNC)
+        # FP16 values widened and offset by w: back to FP16 exactly
+        stored = ((eng.f() - w[:, None]) * 1024.0).astype(np.float16).astype(np.float64)
+    e = np.array([[0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1],
+                  [0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1],
+                  [0, 0, 0, 0, 0, 1, -1, 1, 1, 1, 1, -1, -1, -1, -1]])
+    up = np.zeros((q, n), bool)
+    for i in range(q):
+        vals = np.unique(stored[i])
+        assert 1 <= len(vals) <= 2, (i, vals)
+        v16 = np.float16(exact[i])
+        lo = float(v16) if float(v16) <= exact[i] else float(np.nextafter(v16, np.float16(-np.inf)))
+        hi = float(np.nextafter(np.float16(lo), np.float16(np.inf)))
+        assert set(vals) <= {lo, hi}, (i, vals, lo, hi)
+        p = (exact[i] - lo) / (hi - lo)
+        # node x holds population i as written by node x - e_i: index the
+        # decisions by the node that made them
+        dec = (stored[i] == hi).reshape(64, 64, 64)
+        up[i] = np.roll(dec, (-e[2, i], -e[1, i], -e[0, i]), axis=(0, 1, 2)).reshape(n)
+        frac = up[i].mean()
+        sigma = np.sqrt(max(p * (1 - p), 1e-12) / n)
+        assert abs(frac - p) <= 5 * sigma + 1e-3, (i, frac, p)
+    # independence of the rounding decisions across populations
+    for i, j in [(1, 2), (3, 4), (1, 3), (5, 14), (7, 8), (13, 14)]:
+        a, b = up[i].astype(float), up[j].astype(float)
+        if a.std() > 0 and b.std() > 0:
+            assert abs(np.corrcoef(a, b)[0, 1]) < 0.02, (i, j)
+
+
+def _porous_error(lbmc, storage, ref_u, w, steps):
+    with workloads.engine_for(lbmc, w, storage, streaming=lbmc.STREAM_AA) as eng:
+        eng.iterate(steps, lbmc.STORE_MACROS | lbmc.SYNC)
+        u = eng.u()
+    return (float(np.linalg.norm(u - ref_u) / np.linalg.norm(ref_u)),
+            float(np.abs(u - ref_u).max() / np.abs(ref_u).max()))
+
+
+def test_fp16_sr_porous_velocity_error(lbmc):
+    w = workloads.porous_spheres((128, 64, 32))
+    steps = 2000
+    with workloads.engine_for(lbmc, w, "f64", streaming=lbmc.STREAM_AA) as eng:
+        eng.iterate(steps, lbmc.STORE_MACROS | lbmc.SYNC)
+        ref_u = eng.u()
+    l2_sr, max_sr = _porous_error(lbmc, "f16sr", ref_u, w, steps)
+    l2_rn, max_rn = _porous_error(lbmc, "f16", ref_u, w, steps)
+    print(f"porous 128x64x32, {steps} steps, u error vs FP64: FP16 stochastic L2 {l2_sr:.2e} "
+          f"max {max_sr:.2e}; FP16 nearest L2 {l2_rn:.2e} max {max_rn:.2e}")
+    assert l2_sr <= 1e-3
+    assert l2_sr < l2_rn

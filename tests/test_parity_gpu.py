@@ -21,7 +21,7 @@ from test_oracle_pin import GOLDEN, load_golden
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"f64": 1e-10, "f32": 1e-5, "f16": 5e-3, "bf16": 3e-2}
+TOL = {"f64": 1e-10, "f32": 1e-5, "f16": 5e-3, "f16sr": 5e-3, "bf16": 3e-2}
 
 
 def err(a, b):
@@ -111,17 +111,19 @@ def test_stress_free_faces(lbmc, lat, kernel):
     assert err(ug, ur) <= TOL["f64"]
 
 
-@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("storage", ["f16", "f16sr", "bf16"])
 @pytest.mark.parametrize("lat,ct", [("d2q9", 0), ("d2q9", 3), ("d3q15", 2), ("d3q15", 1)])
-def test_reduced_precision_storage(lbmc, lat, ct, storage):
-    """FP16/BF16 storage; the sizes take the bulk-copy pipeline."""
+def test_reduced_precision_storage(lbmc, lat, ct, storage, kernel):
+    """FP16 (round to nearest and stochastic rounding) and BF16 storage in
+    both step kernels; the sizes let the bulk-copy pipeline take them."""
     length = (40, 24, 1) if lat == "d2q9" else (16, 12, 10)
     case = make_case(lat, length, ct, True, solids=0.05, partial=0.1 if ct % 2 else 0.0,
                      seed=5)
     r = Restatement(case)
     r.run(30)
     rr, ur = r.macros()
-    _, rg, ug = run_engine(lbmc, case, 30, storage)
+    _, rg, ug = run_engine(lbmc, case, 30, storage, kernel=kernel_id(lbmc, kernel))
     assert err(ug, ur) <= TOL[storage]
     assert err(rg - 1, rr - 1) <= TOL[storage]
 
