@@ -43,7 +43,7 @@ sys.path.insert(0, ROOT)
 UNIT = "GLUPS"
 E2E_STEPS = 500
 REF_ARM_SECONDS = 90.0  # bound of one --impl reference run (warm-up + steps)
-STORAGE_BYTES = {"f32": 4, "f16": 2, "bf16": 2, "f64": 8}
+STORAGE_BYTES = {"f32": 4, "f16": 2, "f16sr": 2, "bf16": 2, "f64": 8}
 
 
 def algorithmic_bytes_per_lup(q: int, storage: str) -> int:
@@ -75,23 +75,69 @@ def profiled_traffic(kernel_tag: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region.
+
+    NVML (the library nvidia-smi reads) is polled every 2 ms from a thread,
+    so that a region of a few milliseconds still holds samples; nvidia-smi's
+    100 ms loop is the fallback when NVML cannot be loaded."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_s: float = 0.002):
         self.dev = device_index
+        self.period = period_s
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm_mhz, max_mhz, reasons)
+        self.stop = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _poll(self):
+        nv, h = self.nvml
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(mhz), float(max_mhz),
+                                     {k for k, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            self.stop.wait(self.period)
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.source = "nvml 2 ms"
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi 100 ms"
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -100,9 +146,19 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            parts = [p.strip() for p in line.strip().split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                self.samples.append((float(parts[1]), float(parts[2]),
+                                     {n for n, f in zip(self.REASONS, parts[5:9]) if f.lower() == "active"}))
+            except ValueError:
+                continue
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.nvml is not None:
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -111,24 +167,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        mhz, maxmhz, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                mhz.append(float(parts[1]))
-                maxmhz.append(float(parts[2]))
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower() == "active":
-                    reasons.add(name)
-        if not mhz:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxmhz),
-                "reasons": sorted(reasons), "samples": len(mhz)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": self.source}
+        reasons = set().union(*(r for _, _, r in self.samples))
+        return {"sm_mhz": statistics.median(m for m, _, _ in self.samples),
+                "sm_max_mhz": max(x for _, x, _ in self.samples),
+                "reasons": sorted(reasons), "samples": len(self.samples), "source": self.source}
 
 
 def dist_setup(args):
@@ -226,7 +271,7 @@ def run_batch(args, world, rank, local):
     import workloads
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    tau, g, tol, check = 1.0, 1e-6, 1e-9, 100
+    tau, g, tol, check = BATCH_TAU, BATCH_G, 1e-9, 100
     geoms = workloads.batch_sweep(args.domains, seed=5 + rank, tau=tau)
     nodes = np.array([x.size for x in geoms])
     with lbmc.Batch(geoms[:8], tau=tau, force=(g, 0.0), storage=args.storage) as wb:
@@ -297,6 +342,18 @@ def run_batch(args, world, rank, local):
         alone_conv.append(ok)
         del keep
     both = [i for i, d in enumerate(sample) if conv32[d] and alone_conv[i]]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, desc = reference_batch_rate(geoms, batch_sample(len(geoms)), 200, threads)
+        cpu = {"value": rate / 1e9, "unit": UNIT, "cores": threads, "kind": "reference", "sample": desc}
+    # HBM roofline of the whole run: one read and one write of every
+    # population plus the class byte per lattice update, as for a single
+    # domain; domains held in shared memory read and write HBM once per
+    # launch of K steps, so the run can sit above it.
+    bpl = algorithmic_bytes_per_lup(9, args.storage)
+    peak, peak_kind = measured_peak()
+    achieved = main["glups"] * bpl
     if rank == 0:
         line = {
             "metric": metric_name(args), "value": main["glups"], "unit": UNIT, "n_gpus": world,
@@ -316,6 +373,12 @@ def run_batch(args, world, rank, local):
                 "alone_p50_ms": float(np.percentile(np.array(alone)[both], 50)) if both else None,
                 "alone_p99_ms": float(np.percentile(np.array(alone)[both], 99)) if both else None,
                 "alone_sequential_total_ms": float(np.sum(alone))},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic(f"batch_kernel_sweep16_{args.storage}"),
+                         "peak_source": peak_kind, "bytes_per_lup": bpl,
+                         "kernel": "batch_kernel (persistent, domains from an atomic queue; small domains "
+                                   "K steps per load in shared memory) + batch_wide_kernel (tail phase)"},
+            "cpu_baseline": cpu,
             "gpu_launches": None,
             "clocks": clk.summary(),
         }
@@ -381,8 +444,74 @@ def cpu_reference_rate(w, nz: int, budget_s: float, threads: int):
     return timer.n * steps / t_total, f"{timer.sample}, {steps} steps ({t_total:.1f} s)"
 
 
+BATCH_TAU, BATCH_G = 1.0, 1e-6
+
+
+def _reference_domain(job):
+    """One sweep domain through the host-compiled reference step (a worker
+    process: the reference keeps its DomainConstant in a file-scope global,
+    so one process runs one domain at a time, as LBM-C does)."""
+    geometry, steps = job
+    from oracle.oracle import Case, Reference
+    ly, lx = geometry.shape
+    n = lx * ly
+    if steps == 0:
+        Reference(Case(lattice="d2q9", length=(4, 4, 1)), "asis", nthreads=1).close()
+        return 0
+    force = np.zeros((2, n))
+    force[0] = BATCH_G
+    case = Case(lattice="d2q9", length=(lx, ly, 1), tau=BATCH_TAU, collision_type=1, forcing=True,
+                geometry=geometry.reshape(n), force=force)
+    ref = Reference(case, "asis", nthreads=1)
+    ref.run(steps)
+    ref.close()
+    return n * steps
+
+
+def reference_batch_rate(geoms, sample, steps, threads):
+    """The host-compiled reference step (D2Q9 NTPOR + Guo, FP64) on a sample
+    of the sweep's domains, one domain per worker process and one process
+    per host thread: total lattice updates per second and a description.
+    The pool is spawned (never forked after CUDA use) and warmed up before
+    the timer starts."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    with ProcessPoolExecutor(max_workers=threads, mp_context=mp.get_context("spawn")) as pool:
+        list(pool.map(_reference_domain, [(geoms[0], 0)] * threads))
+        t = time.perf_counter()
+        lups = sum(pool.map(_reference_domain, [(geoms[d], steps) for d in sample]))
+        secs = time.perf_counter() - t
+    nodes = int(sum(geoms[d].size for d in sample))
+    return lups / secs, (f"{len(sample)} seeded domains of the sweep ({nodes} nodes), {steps} steps each, "
+                         f"one domain per process on {threads} host threads, FP64 reference step "
+                         f"({secs:.1f} s)")
+
+
+def batch_sample(ndomains, size=64):
+    return np.random.default_rng(17).choice(ndomains, size=min(size, ndomains), replace=False)
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
+        return
+    if args.workload == "batch":
+        import workloads
+        geoms = workloads.batch_sweep(args.domains, seed=5, tau=BATCH_TAU)
+        threads = os.cpu_count() or 1
+        sample = batch_sample(len(geoms))
+        rate, desc = reference_batch_rate(geoms, sample, max(1, args.steps), threads)
+        value = rate / 1e9
+        line = {"metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded circles, IMB edges)", "impl": "reference",
+                "config": {"workload": "batch_d2q9_ntpor_guo_circles", "domains": args.domains,
+                           "sample": desc, "threads": threads},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                 "sample": desc},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     w = build_workload(args)
     threads = os.cpu_count() or 1
@@ -527,8 +656,13 @@ def run_ours(args, world, rank, local):
                                "fetch": round(t3 - t2, 4), "destroy_untimed": round(t4 - t3, 4)})
         # The slowest job counts.
         e2e_rate, _ = aggregate_rate(w.n * E2E_STEPS, max(times), world, device)
+        # Each job moves its inputs in once and its result out once; per step
+        # that is the job's bytes over its steps.
         e2e = {"value": e2e_rate / 1e9, "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "h2d_bytes_per_step": int(round(h2d / E2E_STEPS)),
+               "d2h_bytes_per_step": int(round(d2h / E2E_STEPS)),
+               "h2d_bytes_per_job": int(h2d), "d2h_bytes_per_job": int(d2h),
+               "steps_per_job": E2E_STEPS,
                "job": f"lbmc_init from host arrays + {E2E_STEPS} steps + fetch rho,u into host arrays"
                       " allocated before the job (lbmc_destroy after the timer, as LBM-C exits without"
                       " freeing); slowest of the timed jobs",

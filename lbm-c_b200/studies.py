@@ -31,7 +31,7 @@ def _timed_iterate(lbmc, eng, steps, flags):
     return time.perf_counter() - t
 
 
-def porous_accuracy(lbmc, L=256, steps=5000, storages=("f64", "f32", "f16", "bf16"),
+def porous_accuracy(lbmc, L=256, steps=5000, storages=("f64", "f32", "f16", "f16sr", "bf16"),
                     streaming=None, log=print):
     w = workloads.porous_spheres((L, L, L))
     streaming = lbmc.STREAM_AA if streaming is None else streaming
@@ -74,7 +74,7 @@ def _enstrophy(torch, u, L):
     return float(0.5 * (wx * wx + wy * wy + wz * wz).mean())
 
 
-def tgv_accuracy(lbmc, torch, L=512, conv_times=20, storages=("f64", "f32", "f16", "bf16"),
+def tgv_accuracy(lbmc, torch, L=512, conv_times=20, storages=("f64", "f32", "f16", "f16sr", "bf16"),
                  streaming=None, log=print):
     w = workloads.taylor_green(L)
     streaming = lbmc.STREAM_AA if streaming is None else streaming
