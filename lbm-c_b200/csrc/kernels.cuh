@@ -176,8 +176,11 @@ __host__ __device__ __forceinline__ unsigned mix32(unsigned x) {
 __host__ __device__ __forceinline__ unsigned sr_step_seed(long long t) {
   return mix32((unsigned)t ^ mix32((unsigned)((unsigned long long)t >> 32) + 0x9e3779b9u));
 }
-// Odd multipliers that turn one hashed word into further random words: the
-// upper half of the 64-bit product h * m_k depends on every bit of h.
+// Odd multipliers that turn one hashed word h into further random words
+// w_k = lo(h m_k) xor hi(h m_k) of the 64-bit product ("multiply-mix": the
+// xor folds the well-mixed upper half into the lower one).  The upper half
+// alone is not uniform in its top bits when m_k is well below 2^32, and the
+// lower half alone ties the low bits of every word to the low bits of h.
 __host__ __device__ constexpr unsigned sr_multiplier(int k) {
   return k == 1 ? 0x9e3779b1u : k == 2 ? 0x85ebca77u : k == 3 ? 0xc2b2ae3du : k == 4 ? 0x27d4eb2fu
        : k == 5 ? 0x165667b1u : k == 6 ? 0xd3a2646du : 0xfd7046c5u;
@@ -193,9 +196,14 @@ __device__ __forceinline__ unsigned cvt_rs_f16x2(float hi, float lo, unsigned rb
   return d;
 }
 
+__host__ __device__ __forceinline__ unsigned sr_word(unsigned h, int k) {
+  const unsigned long long p = (unsigned long long)h * sr_multiplier(k);
+  return (unsigned)p ^ (unsigned)(p >> 32);
+}
+
 // Writes a node's Q post-collision values with stochastic rounding, two per
 // conversion: population pair (2k, 2k+1) takes random word k, word 0 being
-// mix32(node ^ step seed) and word k > 0 its product with sr_multiplier(k).
+// h = mix32(node ^ step seed) and word k > 0 sr_word(h, k).
 // The bits depend only on (node, step, population), so every streaming
 // layout writes the same values.  ptr(ic) is the destination of population
 // ic; GLOBAL selects the streaming-hint global store (else a plain store,
@@ -210,7 +218,7 @@ __device__ __forceinline__ void store_node_sr(const float (&out)[Q], float scale
   unroll<(Q + 1) / 2>([&](auto pc) {
     constexpr int k = decltype(pc)::value;
     constexpr int i0 = 2 * k, i1 = 2 * k + 1;
-    const unsigned r = k == 0 ? h : __umulhi(h, sr_multiplier(k));
+    const unsigned r = k == 0 ? h : sr_word(h, k);
     float hi = 0.0f;
     if constexpr (i1 < Q) hi = out[i1] * scale;
     const unsigned d = cvt_rs_f16x2(hi, out[i0] * scale, r);

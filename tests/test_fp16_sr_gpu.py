@@ -32,7 +32,9 @@ def test_stochastic_rounding_is_unbiased(lbmc):
     w = np.array([2 / 9] + [1 / 9] * 6 + [1 / 72] * 8)
     rho0, u0 = 1.0 + 3.1e-4, np.array([1.7e-3, -0.9e-3, 0.4e-3])
     r = Restatement(case)
-    case.f0 = np.repeat(r.equilibrium(np.full(1, rho0), u0[:, None]), n, axis=1)
+    f0 = r.equilibrium(np.full(n, rho0), np.tile(u0[:, None], (1, n)))
+    # the state the engine starts from: f - w as uploaded (FP16, x 1024)
+    case.f0 = w[:, None] + ((f0 - w[:, None]) * 1024.0).astype(np.float16).astype(np.float64) / 1024.0
     case.force = np.tile(np.array([2.3e-5, 1.1e-5, -0.7e-5])[:, None], (1, n))
     case.geometry = np.zeros(n)
     r = Restatement(case)
