@@ -279,7 +279,7 @@ def run_batch(args, world, rank, local):
 
     def batched(storage, cap):
         torch.cuda.synchronize(dev)
-        b = lbmc.Batch(geoms, tau=tau, force=(g, 0.0), storage=storage)
+        b = lbmc.Batch(geoms, tau=tau, force=(g, 0.0), storage=storage, wide_below=args.wide_below)
         t1 = time.perf_counter()
         res = b.run(cap, tol, check)
         torch.cuda.synchronize(dev)
@@ -724,6 +724,9 @@ def main():
     ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
     ap.add_argument("--domains", type=int, default=4096)
     ap.add_argument("--batch-cap", type=int, default=20000)
+    ap.add_argument("--wide-below", type=int, default=0,
+                    help="batched sweep: step the HBM domains over every SM once fewer than this "
+                         "many run (0 = half the SMs, -1 = never)")
     ap.add_argument("--alone-sample", type=int, default=32)
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")

@@ -267,7 +267,7 @@ typedef struct lbmc_batch_config {
 } lbmc_batch_config;
 
 typedef struct lbmc_batch_domain {
-  int length[2];            /* Lx, Ly */
+  int length[2];            /* Lx, Ly; Lx * Ly <= 2^24 */
   const double *geometry;   /* Lx*Ly Porosity B: 0 fluid, (0,1) partial, >= 1 solid; NULL = fluid */
 } lbmc_batch_domain;
 

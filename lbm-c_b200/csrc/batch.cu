@@ -204,13 +204,21 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
       const bool save = (t % A.check) == 0;
       const bool test = save && t >= A.check;
       float dmax = 0;
+      // (x, y) of node k advance by the block size without a division per node.
+      int x = (int)threadIdx.x % D.lx, y = (int)threadIdx.x / D.lx;
+      const int step_x = (int)blockDim.x % D.lx, step_y = (int)blockDim.x / D.lx;
       for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int x = k % D.lx, y = k / D.lx;
         const int c = cls[k];
         float ux, uy;
         batch_node<S, BLEND>(pop, pitch, k, x, y, D.lx, D.ly, sx, sy, c, a, ux, uy);
         if (test) dmax = nan_max(dmax, node_delta(ux, uy, up[k]));
         if (save) up[k] = make_float2(ux, uy);
+        x += step_x;
+        y += step_y;
+        if (x >= D.lx) {
+          x -= D.lx;
+          y += 1;
+        }
       }
       __syncthreads();
       if (test) {
@@ -246,6 +254,16 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
 }
 
 __global__ void stamp_kernel(unsigned long long *out) { *out = global_ns(); }
+
+// k / d for 0 <= k < 2^24 (every batched domain has fewer nodes) and
+// d >= 1 through an FP32 reciprocal: both roundings are toward zero, so the
+// FP32 quotient is at most the true one and, since k/d < 2^22 whenever
+// d > 2 (d <= 2 divides exactly), less than 1 below it; one correction.
+__device__ __forceinline__ int div_small(int k, int d) {
+  int q = (int)__fmul_rz((float)k, __frcp_rz((float)d));
+  if (k - q * d >= d) q += 1;
+  return q;
+}
 
 // Tail phase: one step of the listed domains, a 256-node tile per block
 // (grid-stride over the tiles).  The convergence test's block maxima go to
@@ -284,7 +302,8 @@ __global__ void __launch_bounds__(WIDE_THREADS)
     float dmax = 0;
     if (k < n) {
       float ux, uy;
-      batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, k % D.lx, k / D.lx, D.lx, D.ly, sx, sy,
+      const int y = div_small(k, D.lx), x = k - y * D.lx;
+      batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, y, D.lx, D.ly, sx, sy,
                            A.cls[D.node_off + k], a, ux, uy);
       if (test) dmax = node_delta(ux, uy, up[k]);
       if (save) up[k] = make_float2(ux, uy);
@@ -563,7 +582,7 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   b->dom.resize(ndomains);
   for (int d = 0; d < ndomains; d++) {
     const int lx = doms[d].length[0], ly = doms[d].length[1];
-    if (lx < 1 || ly < 1 || (long long)lx * ly > (1LL << 30)) {
+    if (lx < 1 || ly < 1 || (long long)lx * ly > (1LL << 24)) {
       delete b;
       return berr(LBMC_ERR_INVALID_ARG, "domain " + std::to_string(d) + " has a bad size");
     }
