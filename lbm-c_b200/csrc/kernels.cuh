@@ -292,6 +292,8 @@ struct StepArgs {
   int odd;   // AA: the current step is odd
   int n;
   C tau;
+  C omega;    // 1/tau
+  C guo_pre;  // Guo prefactor 1 - 1/(2 tau)
   C s_mrt[15];
   C c_smag;
   C scale, inv_scale;
@@ -470,6 +472,22 @@ __device__ __forceinline__ C edot(const C *v) {
   return r;
 }
 
+// 1/x for the per-node reciprocals (density, local relaxation time): FP32
+// uses the hardware approximation (rcp.approx.ftz.f32, at most 1 ulp from
+// the rounded quotient, one instruction instead of the IEEE division's
+// sequence); FP64 divides exactly.  Uniform reciprocals (1/tau, the Guo
+// prefactor) come from the host in StepArgs.
+template <class C>
+__device__ __forceinline__ C recip(C x) {
+  if constexpr (std::is_same<C, float>::value) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  } else {
+    return C(1) / x;
+  }
+}
+
 // rho = 1 + sum g, u = sum e g / rho (LBM-C/solver.cu:96-108).
 template <class L, class C>
 __device__ __forceinline__ void moments(Node<L, C> &nd) {
@@ -485,7 +503,7 @@ __device__ __forceinline__ void moments(Node<L, C> &nd) {
   });
   nd.drho = d;
   nd.rho = C(1) + d;
-  const C inv = C(1) / nd.rho;
+  const C inv = recip(nd.rho);
   nd.u[0] = jx * inv;
   nd.u[1] = jy * inv;
   nd.u[2] = L::DIM > 2 ? jz * inv : C(0);
@@ -836,11 +854,11 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       F[2] = a.force_u[2];
     }
     // u <- u + F/(2 rho) (collision.cu:74-78)
-    const C h = C(1) / (C(2) * nd.rho);
+    const C h = C(0.5) * recip(nd.rho);
     nd.u[0] += h * F[0];
     nd.u[1] += h * F[1];
     if (L::DIM > 2) nd.u[2] += h * F[2];
-    pre = C(1) - C(1) / (C(2) * tau0);
+    pre = a.guo_pre;  // 1 - 1/(2 tau)
     uF = nd.u[0] * F[0] + nd.u[1] * F[1] + (L::DIM > 2 ? nd.u[2] * F[2] : C(0));
   }
   const C omb = C(1) - B;
@@ -996,7 +1014,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       const C r2 = sqrt(C(2));
       C qhat = r2 * (fabs(q[0]) + fabs(q[1]) + C(2) * fabs(q[3]));
       if (L::DIM > 2) qhat += r2 * (fabs(q[2]) + C(2) * (fabs(q[4]) + fabs(q[5])));
-      const C k = C(2) * r2 * a.c_smag * a.c_smag * (C(9) / nd.rho);
+      const C k = C(2) * r2 * a.c_smag * a.c_smag * (C(9) * recip(nd.rho));
       const C tau_smag = tau0 + C(0.5) * (sqrt(tau0 * tau0 + k * qhat) - tau0);
       if constexpr (COL == COL_BGK_SMAG) {
         tau = tau_smag;
@@ -1031,7 +1049,8 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
         tau = in_range ? tau_l : tau_smag;
       }
     }
-    const C om = C(1) / tau;
+    // 1/tau: the host's value for a uniform tau, else the local one
+    const C om = (COL == COL_BGK_SMAG || COL == COL_BGK_MLP) ? recip(tau) : a.omega;
     // population 0 (e = 0)
     out[0] = nd.g[0] - omb * (om * (nd.g[0] - A0)) + omb * ft0e;
     unroll<L::NP>([&](auto pc) {
