@@ -76,7 +76,7 @@ struct BatchArgs {
   float tol;
   long long max_steps;
   float tau, force[2];
-  float omega, guo_pre;      // 1/tau and 1 - 1/(2 tau)
+  float omega;               // 1/tau
   float scale, inv_scale;
   int blend;
   size_t smem_elems;         // capacity of the shared-memory population buffer
@@ -167,7 +167,6 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
   memset(&a, 0, sizeof(a));
   a.tau = A.tau;
   a.omega = A.omega;
-  a.guo_pre = A.guo_pre;
   a.force_u[0] = A.force[0];
   a.force_u[1] = A.force[1];
   a.scale = A.scale;
@@ -286,7 +285,6 @@ __global__ void __launch_bounds__(WIDE_THREADS)
   memset(&a, 0, sizeof(a));
   a.tau = A.tau;
   a.omega = A.omega;
-  a.guo_pre = A.guo_pre;
   a.force_u[0] = A.force[0];
   a.force_u[1] = A.force[1];
   a.scale = A.scale;
@@ -448,7 +446,6 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
   A.max_steps = max_steps;
   A.tau = (float)b->cfg.tau;
   A.omega = (float)(1.0 / b->cfg.tau);
-  A.guo_pre = (float)(1.0 - 1.0 / (2.0 * b->cfg.tau));
   A.force[0] = (float)b->cfg.force[0];
   A.force[1] = (float)b->cfg.force[1];
   A.scale = (float)b->scale;

@@ -293,7 +293,6 @@ struct StepArgs {
   int n;
   C tau;
   C omega;    // 1/tau
-  C guo_pre;  // Guo prefactor 1 - 1/(2 tau)
   C s_mrt[15];
   C c_smag;
   C scale, inv_scale;
@@ -475,8 +474,8 @@ __device__ __forceinline__ C edot(const C *v) {
 // 1/x for the per-node reciprocals (density, local relaxation time): FP32
 // uses the hardware approximation (rcp.approx.ftz.f32, at most 1 ulp from
 // the rounded quotient, one instruction instead of the IEEE division's
-// sequence); FP64 divides exactly.  Uniform reciprocals (1/tau, the Guo
-// prefactor) come from the host in StepArgs.
+// sequence); FP64 divides exactly.  1/tau for a uniform tau comes from the
+// host in StepArgs.
 template <class C>
 __device__ __forceinline__ C recip(C x) {
   if constexpr (std::is_same<C, float>::value) {
@@ -854,11 +853,11 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       F[2] = a.force_u[2];
     }
     // u <- u + F/(2 rho) (collision.cu:74-78)
-    const C h = C(0.5) * recip(nd.rho);
+    const C h = recip(C(2) * nd.rho);
     nd.u[0] += h * F[0];
     nd.u[1] += h * F[1];
     if (L::DIM > 2) nd.u[2] += h * F[2];
-    pre = a.guo_pre;  // 1 - 1/(2 tau)
+    pre = C(1) - recip(C(2) * tau0);
     uF = nd.u[0] * F[0] + nd.u[1] * F[1] + (L::DIM > 2 ? nd.u[2] * F[2] : C(0));
   }
   const C omb = C(1) - B;
