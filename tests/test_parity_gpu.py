@@ -253,13 +253,20 @@ def test_init_large_is_exact_and_repeatable(lbmc, length, init):
 
 @pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
 def test_pipelined_and_direct_kernels_agree(lbmc, storage):
-    """The two step kernels compute the same thing: identical bits."""
+    """The two step kernels run the same collision code: identical bits with
+    FP32 and FP16 storage.  In FP64 the compiler may fuse a multiply and an
+    add into one FMA in one kernel and not in the other (the two inline the
+    collision into different surroundings), so they agree to a few units in
+    the last place (4e-16 relative to the largest value after 25 steps)."""
     case = make_case("d3q15", (32, 20, 12), 3, True, solids=0.1, partial=0.1, micro="zh",
                      macro="random", seed=12)
     a = run_engine(lbmc, case, 25, storage, kernel=lbmc.KERNEL_DIRECT)
     b = run_engine(lbmc, case, 25, storage, kernel=lbmc.KERNEL_PIPELINED)
     for x, y in zip(a, b):
-        np.testing.assert_array_equal(x, y)
+        if storage == "f64":
+            assert np.abs(x - y).max() <= 4e-16 * np.abs(y).max()
+        else:
+            np.testing.assert_array_equal(x, y)
 
 
 def test_pipelined_rejects_ragged_rows(lbmc):
