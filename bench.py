@@ -726,7 +726,7 @@ def main():
     ap.add_argument("--batch-cap", type=int, default=20000)
     ap.add_argument("--wide-below", type=int, default=0,
                     help="batched sweep: step the HBM domains over every SM once fewer than this "
-                         "many run (0 = half the SMs, -1 = never)")
+                         "many run (0 = from the start, -1 = never: one block per domain)")
     ap.add_argument("--alone-sample", type=int, default=32)
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")

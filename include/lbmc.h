@@ -260,9 +260,10 @@ typedef struct lbmc_batch_config {
   int device;
   int block_threads;    /* 0 = autotune (256/512/1024) */
   int steps_per_launch; /* 0 = autotune (check_every or 4*check_every) */
-  int wide_below;       /* tail phase: once fewer than this many domains stepped in HBM are
-                           still running, each step spreads them over every SM instead of one
-                           block per domain; 0 = default (half the SMs), < 0 = never */
+  int wide_below;       /* domains too large for shared memory are stepped one step per launch
+                           over every SM once fewer than this many of them are running, and
+                           before that one block per domain, K steps per launch; 0 = default
+                           (over every SM from the start), < 0 = never */
   int reserved[7];
 } lbmc_batch_config;
 

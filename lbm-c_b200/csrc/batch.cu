@@ -3,33 +3,34 @@
 // process; each domain here is stepped exactly as lbmc_iterate steps a single
 // domain (same shift layout, same collide_fluid), so parity is inherited.
 //
-// Execution model.  One persistent kernel launch advances every unconverged
-// domain by up to K steps.  Blocks take domains from an atomic queue (domains
-// sorted by size, largest first); a whole domain belongs to one block, so the
-// step-to-step dependency is a __syncthreads, not a grid barrier.  A domain
-// whose populations fit in the block's shared memory is loaded once, stepped
-// K times in shared memory and written back, so its K steps cost one read and
-// one write of HBM; larger domains are stepped in HBM.  Every C steps a
-// domain compares u with the previous step (max norm) and freezes once below
-// the tolerance, recording the device timer.  Shared-memory-resident domains
-// and HBM domains run in two kernels launched as parallel branches of the
-// graph, each with its own queue and launch shape.  The host replays a CUDA graph
-// (queue reset + kernel) until all domains converged or hit the step cap.  An
-// autotuner times the first launches with several block sizes and K, keeps
-// the fastest.
+// Execution model.  Domains whose populations fit in a block's shared
+// memory are stepped by one persistent kernel: blocks take whole domains
+// from an atomic queue (largest first), load one, step it K times in shared
+// memory (the step-to-step dependency is a __syncthreads) and write it back,
+// so K steps cost one read and one write of HBM.  Domains too large for
+// shared memory are stepped in HBM one step per launch over every SM
+// (batch_wide_kernel: one warp per 32-node row segment, all running HBM
+// domains in one launch), followed by a one-thread-per-domain kernel
+// (batch_wide_finish_kernel) for the convergence test and step accounting;
+// K such step pairs run in a second branch of the same CUDA graph.  Every C
+// steps a domain compares u with its value C steps earlier (max norm) and
+// freezes once below the tolerance, recording the device timer.  The host
+// replays the graph until every domain converged, stopped or hit the step
+// cap; once a quarter of the listed HBM domains have stopped, their row
+// segments are rebuilt and the graph re-captured, so launches stop visiting
+// them.  An autotuner times the first launches with several block sizes for
+// the shared-memory kernel and two values of K, and keeps the fastest.
 //
-// Tail phase.  One block per domain leaves SMs idle once fewer HBM domains
-// are running than there are blocks, and the largest domains, which need the
-// most steps, finish last on one SM each.  When fewer than `wide_below`
-// HBM domains are still running, the host switches them to a second graph
-// whose side branch steps them one step per launch over every SM (256-node
-// tiles, batch_wide_kernel) followed by a one-thread-per-domain kernel
-// (batch_wide_finish_kernel) that applies the same convergence test and step
-// accounting as batch_kernel; the same node update runs in both phases, so
-// results do not depend on the phase a step ran in.
+// The HBM domains can also run in the persistent kernel, one block per
+// domain, K steps per launch (lbmc_batch_config.wide_below < 0, or until
+// fewer than wide_below remain): that design leaves SMs idle when few large
+// domains are running (measured: 64 domains of 512 x 512 at 11 GLUPS against
+// 53 GLUPS over every SM).  The same node update runs in both kernels, so
+// results do not depend on where a step ran.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -112,9 +113,14 @@ __device__ __forceinline__ void batch_node(S *pop, long long pitch, int k, int x
     // a.B is this domain's porosity array; only partial nodes read it.
     collide_fluid<L, float, COL_BGK, true, BLEND>(nd, a, k, cls == 2 ? ENTRY_PARTIAL : 0u, out);
   }
+  // The store slots equal the load slots; recomputing them from the six
+  // coordinates is cheaper than keeping nine addresses live across the
+  // collision (the empty asm hides the equality from the compiler).
+  int xw[3] = {xs[0], xs[1], xs[2]}, yw[3] = {ys[0], ys[1], ys[2]};
+  asm("" : "+r"(xw[0]), "+r"(xw[1]), "+r"(xw[2]), "+r"(yw[0]), "+r"(yw[1]), "+r"(yw[2]));
   unroll<9>([&](auto ic) {
     constexpr int i = decltype(ic)::value;
-    const int slot = xs[sel(L::e(0, i))] + lx * ys[sel(L::e(1, i))];
+    const int slot = xw[sel(L::e(0, i))] + lx * yw[sel(L::e(1, i))];
     store_smem(pop + i * pitch + slot, out[i], a.scale);
   });
   ux = nd.u[0];
@@ -257,29 +263,35 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
 
 __global__ void stamp_kernel(unsigned long long *out) { *out = global_ns(); }
 
-// k / d for 0 <= k < 2^24 (every batched domain has fewer nodes) and
-// d >= 1 through an FP32 reciprocal: both roundings are toward zero, so the
-// FP32 quotient is at most the true one and, since k/d < 2^22 whenever
-// d > 2 (d <= 2 divides exactly), less than 1 below it; one correction.
-__device__ __forceinline__ int div_small(int k, int d) {
-  int q = (int)__fmul_rz((float)k, __frcp_rz((float)d));
-  if (k - q * d >= d) q += 1;
-  return q;
-}
-
-// Tail phase: one step of the listed domains, a 256-node tile per block
-// (grid-stride over the tiles).  The convergence test's block maxima go to
-// acc[domain] (non-negative floats compare as their bit patterns, and the
-// positive NaN of a non-finite velocity is above every one of them).
-constexpr int WIDE_THREADS = 256;
-struct WideTile {
-  int domain, first;
+// Wide phase: one step of the listed HBM domains per launch over every SM.
+// The work is cut into row segments of 32 nodes (domain, row y, first x),
+// one per warp, two warps per block, one block per two segments: x is the
+// lane's offset in the segment and y is uniform, so no node index is
+// divided, and the row offsets of the shift layout are warp-uniform.  A
+// row whose length is not a multiple of 32 leaves lanes of its last segment
+// idle.  The convergence test's warp maxima go to acc[domain] (non-negative
+// floats compare as their bit patterns, and the positive NaN of a
+// non-finite velocity is above every one of them).
+constexpr int WIDE_THREADS = 64;
+constexpr int WIDE_WARPS = WIDE_THREADS / 32;
+struct RowSegment {
+  int domain, y, x0;
 };
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
 
 template <class S, bool BLEND>
 __global__ void __launch_bounds__(WIDE_THREADS)
-    batch_wide_kernel(const BatchArgs A, const WideTile *tiles, int ntiles, int *acc) {
-  __shared__ float sh_red[32];
+    batch_wide_kernel(const BatchArgs A, const RowSegment *segs, int nsegs, int *acc) {
+  const int si = blockIdx.x * WIDE_WARPS + (int)(threadIdx.x >> 5);
+  if (si >= nsegs) return;  // whole warps
+  const RowSegment G = segs[si];
+  const BatchStateDev &st = A.state[G.domain];
+  if (st.converged) return;  // warp-uniform: one domain per segment
   S *pool = reinterpret_cast<S *>(A.pool);
   StepArgs<float> a;
   memset(&a, 0, sizeof(a));
@@ -289,32 +301,26 @@ __global__ void __launch_bounds__(WIDE_THREADS)
   a.force_u[1] = A.force[1];
   a.scale = A.scale;
   a.inv_scale = A.inv_scale;
-  for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
-    const WideTile T = tiles[ti];
-    const BatchStateDev &st = A.state[T.domain];
-    if (st.converged) continue;  // the whole block: one domain per tile
-    const BatchDomainDev D = A.dom[T.domain];
-    const int n = D.lx * D.ly;
-    const long long t = st.t;
-    const int sx = (int)(t % D.lx), sy = (int)(t % D.ly);
-    const bool save = (t % A.check) == 0;
-    const bool test = save && t >= A.check;
-    a.B = A.B + D.node_off;
+  const BatchDomainDev D = A.dom[G.domain];
+  const long long t = st.t;
+  const int sx = (int)(t % D.lx), sy = (int)(t % D.ly);
+  const bool save = (t % A.check) == 0;
+  const bool test = save && t >= A.check;
+  a.B = A.B + D.node_off;
+  const int x = G.x0 + (int)(threadIdx.x & 31);
+  float dmax = 0;
+  if (x < D.lx) {
+    const int k = x + G.y * D.lx;
     float2 *up = A.u_prev + D.node_off;
-    const int k = T.first + (int)threadIdx.x;
-    float dmax = 0;
-    if (k < n) {
-      float ux, uy;
-      const int y = div_small(k, D.lx), x = k - y * D.lx;
-      batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, y, D.lx, D.ly, sx, sy,
-                           A.cls[D.node_off + k], a, ux, uy);
-      if (test) dmax = node_delta(ux, uy, up[k]);
-      if (save) up[k] = make_float2(ux, uy);
-    }
-    if (test) {
-      const float m = block_max(dmax, sh_red);
-      if (threadIdx.x == 0) atomicMax(acc + T.domain, __float_as_int(m));
-    }
+    float ux, uy;
+    batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, G.y, D.lx, D.ly, sx, sy, A.cls[D.node_off + k], a,
+                         ux, uy);
+    if (test) dmax = node_delta(ux, uy, up[k]);
+    if (save) up[k] = make_float2(ux, uy);
+  }
+  if (test) {
+    const float m = warp_max(dmax);
+    if ((threadIdx.x & 31) == 0) atomicMax(acc + G.domain, __float_as_int(m));
   }
 }
 
@@ -471,9 +477,16 @@ cudaError_t enqueue(lbmc_batch *b, int steps, int check, double tol, long long m
 // Tail phase: the listed HBM domains on every SM (per step: tiles, then the
 // per-domain finish), resident domains as before, in two graph branches.
 struct WideWork {
-  WideTile *tiles = nullptr;
+  RowSegment *segs = nullptr;
   int *wide = nullptr;
-  int ntiles = 0, nwide = 0, grid = 1;
+  int nsegs = 0, nwide = 0;
+  void release() {
+    if (segs) cudaFree(segs);
+    if (wide) cudaFree(wide);
+    segs = nullptr;
+    wide = nullptr;
+    nsegs = nwide = 0;
+  }
 };
 
 template <class S>
@@ -487,9 +500,11 @@ cudaError_t launch_wide(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hb
     kr<<<b->sms, threads, b->smem_bytes, st>>>(res);
   }
   auto kw = b->blend ? batch_wide_kernel<S, true> : batch_wide_kernel<S, false>;
+  const unsigned grid = (unsigned)((w.nsegs + WIDE_WARPS - 1) / WIDE_WARPS);
   for (int s = 0; s < hbm.steps; s++) {
-    kw<<<w.grid, WIDE_THREADS, 0, b->side>>>(hbm, w.tiles, w.ntiles, b->acc);
-    batch_wide_finish_kernel<<<(w.nwide + 127) / 128, 128, 0, b->side>>>(hbm, w.wide, w.nwide, b->acc,
+    if (grid > 0) kw<<<grid, WIDE_THREADS, 0, b->side>>>(hbm, w.segs, w.nsegs, b->acc);
+    if (w.nwide > 0)
+      batch_wide_finish_kernel<<<(w.nwide + 127) / 128, 128, 0, b->side>>>(hbm, w.wide, w.nwide, b->acc,
                                                                         s == hbm.steps - 1);
   }
   e = cudaGetLastError();
@@ -511,44 +526,30 @@ cudaError_t enqueue_wide(lbmc_batch *b, int steps, int check, double tol, long l
   }
 }
 
-template <class S>
-cudaError_t wide_occupancy(bool blend, int &per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, blend ? batch_wide_kernel<S, true> : batch_wide_kernel<S, false>, WIDE_THREADS, 0);
-}
-
-// The HBM domains still running, as tiles; device arrays in w (caller frees).
+// The HBM domains still running, as row segments; device arrays in w (the
+// caller releases them).
 cudaError_t build_wide(lbmc_batch *b, WideWork &w) {
   std::vector<BatchStateDev> st(b->ndomains);
   cudaError_t e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return e;
-  std::vector<WideTile> tiles;
+  std::vector<RowSegment> segs;
   std::vector<int> wide;
   for (int d : b->order) {
     const BatchDomainDev &D = b->dom[d];
     if (D.resident || st[d].converged) continue;
     wide.push_back(d);
-    const int n = D.lx * D.ly;
-    for (int first = 0; first < n; first += WIDE_THREADS) tiles.push_back({d, first});
+    for (int y = 0; y < D.ly; y++)
+      for (int x0 = 0; x0 < D.lx; x0 += 32) segs.push_back({d, y, x0});
   }
-  w.ntiles = (int)tiles.size();
+  w.nsegs = (int)segs.size();
   w.nwide = (int)wide.size();
-  e = cudaMalloc(&w.tiles, sizeof(WideTile) * std::max(1, w.ntiles));
+  e = cudaMalloc(&w.segs, sizeof(RowSegment) * std::max(1, w.nsegs));
   if (e == cudaSuccess) e = cudaMalloc(&w.wide, sizeof(int) * std::max(1, w.nwide));
-  if (e == cudaSuccess && w.ntiles)
-    e = cudaMemcpy(w.tiles, tiles.data(), sizeof(WideTile) * w.ntiles, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && w.nsegs)
+    e = cudaMemcpy(w.segs, segs.data(), sizeof(RowSegment) * w.nsegs, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && w.nwide) e = cudaMemcpy(w.wide, wide.data(), sizeof(int) * w.nwide, cudaMemcpyHostToDevice);
-  int per_sm = 0;
-  if (e == cudaSuccess) {
-    switch (b->cfg.storage) {
-      case LBMC_F16: e = wide_occupancy<__half>(b->blend, per_sm); break;
-      case LBMC_BF16: e = wide_occupancy<__nv_bfloat16>(b->blend, per_sm); break;
-      default: e = wide_occupancy<float>(b->blend, per_sm); break;
-    }
-  }
   // Pageable copies above: make sure they landed before the side stream reads.
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
-  w.grid = std::max(1, std::min(w.ntiles, b->sms * std::max(1, per_sm)));
   return e;
 }
 
@@ -672,7 +673,7 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   }
   b->threads = cfg->block_threads;
   b->steps = cfg->steps_per_launch;
-  b->wide_below = cfg->wide_below == 0 ? b->sms / 2 : cfg->wide_below;
+  b->wide_below = cfg->wide_below == 0 ? INT_MAX : cfg->wide_below;
   *out = b;
   return LBMC_OK;
 }
@@ -684,6 +685,30 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
   if (cudaSetDevice(b->cfg.device) != cudaSuccess) return berr(LBMC_ERR_CUDA, "cudaSetDevice");
   cudaError_t e = cudaSuccess;
   stamp_kernel<<<1, 1, 0, b->stream>>>(b->t0);
+
+  // The wide phase (HBM domains stepped over every SM) starts once fewer
+  // than wide_below HBM domains are running: at once with the default.
+  WideWork w;
+  bool wide = false;
+  if (b->wide_below > 0) {
+    std::vector<BatchStateDev> st(b->ndomains);
+    e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
+    long long hbm_active = 0;
+    for (int d = 0; d < b->ndomains; d++) hbm_active += !b->dom[d].resident && !st[d].converged;
+    if (hbm_active > 0 && hbm_active < b->wide_below) {
+      e = build_wide(b, w);
+      if (e != cudaSuccess) {
+        w.release();
+        return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
+      }
+      wide = true;
+    }
+  }
+  auto enqueue_any = [&](int steps, int threads) {
+    return wide ? enqueue_wide(b, steps, check_every, tol, max_steps, threads, w, b->stream)
+                : enqueue(b, steps, check_every, tol, max_steps, threads, b->stream);
+  };
 
   // Autotune the launch shape on the first launches (they are real steps).
   if (b->threads <= 0 || b->steps <= 0) {
@@ -699,7 +724,7 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
         const int th = b->threads > 0 ? b->threads : cand_threads[ti];
         const int sp = b->steps > 0 ? b->steps : cand_steps[si];
         cudaEventRecord(e0, b->stream);
-        e = enqueue(b, sp, check_every, tol, max_steps, th, b->stream);
+        e = enqueue_any(sp, th);
         cudaEventRecord(e1, b->stream);
         if (e == cudaSuccess) e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) break;
@@ -714,57 +739,56 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
       }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+      w.release();
+      return berr(LBMC_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    }
     b->threads = bt;
     b->steps = bs;
   }
 
-  // Capture one launch (queue reset + both kernels) in a graph and replay it;
-  // once few HBM domains remain, switch them to the tail-phase graph.
-  auto capture = [&](auto enqueue_fn, cudaGraph_t &graph, cudaGraphExec_t &exec) -> cudaError_t {
+  // Capture one launch (queue reset + the kernels of K steps) in a graph and
+  // replay it.  In the wide phase the graph holds the row segments of the
+  // HBM domains still running; once a quarter of them have stopped, the
+  // segments are rebuilt so that launches no longer visit stopped domains.
+  auto capture = [&](cudaGraph_t &graph, cudaGraphExec_t &exec) -> cudaError_t {
     cudaError_t ec = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (ec != cudaSuccess) return ec;
-    cudaError_t e2 = enqueue_fn();
+    cudaError_t e2 = enqueue_any(b->steps, b->threads);
     ec = cudaStreamEndCapture(b->stream, &graph);
     if (e2 != cudaSuccess) ec = e2;
     if (ec == cudaSuccess) ec = cudaGraphInstantiate(&exec, graph, 0);
     return ec;
   };
-  cudaGraph_t graph = nullptr, graph_w = nullptr;
-  cudaGraphExec_t exec = nullptr, exec_w = nullptr;
-  WideWork w;
-  bool wide = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  auto drop_graph = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  };
   auto go_wide = [&]() -> cudaError_t {
+    drop_graph();
+    w.release();
     cudaError_t ew = build_wide(b, w);
-    if (ew == cudaSuccess)
-      ew = capture([&] { return enqueue_wide(b, b->steps, check_every, tol, max_steps, b->threads, w, b->stream); },
-                   graph_w, exec_w);
     wide = ew == cudaSuccess;
+    if (ew == cudaSuccess) ew = capture(graph, exec);
     return ew;
   };
-  e = capture([&] { return enqueue(b, b->steps, check_every, tol, max_steps, b->threads, b->stream); }, graph, exec);
+  if (e == cudaSuccess) e = capture(graph, exec);
   int counts[4] = {0, 0, 1, 0};
-  if (e == cudaSuccess && b->wide_below > 0) {
-    // Already few HBM domains running (a small batch, or after earlier runs).
-    std::vector<BatchStateDev> st(b->ndomains);
-    e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
-    int hbm_active = 0;
-    for (int d = 0; d < b->ndomains; d++) hbm_active += !b->dom[d].resident && !st[d].converged;
-    if (e == cudaSuccess && hbm_active > 0 && hbm_active < b->wide_below) e = go_wide();
-  }
   const long long launches_max = max_steps / std::max(1, b->steps) + 2;
   for (long long l = 0; e == cudaSuccess && counts[2] > 0 && l < launches_max; l++) {
-    e = cudaGraphLaunch(wide ? exec_w : exec, b->stream);
+    e = cudaGraphLaunch(exec, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(counts, b->counters, sizeof(counts), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-    if (e == cudaSuccess && !wide && b->wide_below > 0 && counts[3] > 0 && counts[3] < b->wide_below) e = go_wide();
+    if (e != cudaSuccess || counts[2] == 0) break;
+    if (!wide && b->wide_below > 0 && counts[3] > 0 && counts[3] < b->wide_below) e = go_wide();
+    else if (wide && counts[3] > 0 && 4LL * counts[3] < 3LL * w.nwide) e = go_wide();
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
-  if (exec_w) cudaGraphExecDestroy(exec_w);
-  if (graph_w) cudaGraphDestroy(graph_w);
-  if (w.tiles) cudaFree(w.tiles);
-  if (w.wide) cudaFree(w.wide);
+  drop_graph();
+  w.release();
   if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
   if (results) {
     std::vector<BatchStateDev> st(b->ndomains);

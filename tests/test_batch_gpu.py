@@ -72,15 +72,16 @@ def test_batch_converges_and_freezes(lbmc):
 # tolerance above it lets its domains converge too.
 @pytest.mark.parametrize("storage,tol,cap", [("f32", 1e-9, 200000), ("f16", 1e-5, 50000)])
 def test_batch_tail_phase_is_bit_identical(lbmc, storage, tol, cap):
-    """The tail phase (HBM domains spread over every SM, one step per launch)
-    and the one-domain-per-block phase run the same node update and the same
-    convergence rule, so a batch run to steady state never in the tail phase,
-    wholly in it, or switching to it once fewer than 3 HBM domains are left,
-    ends bit for bit the same: step counts, convergence, last delta_u and
-    populations."""
+    """The wide phase (HBM domains spread over every SM, one step per launch,
+    row segments rebuilt as domains stop) and the one-domain-per-block phase
+    run the same node update and the same convergence rule, so a batch run to
+    steady state never in the wide phase, wholly in it (the default, and an
+    explicit threshold), or switching to it once fewer than 3 HBM domains are
+    left, ends bit for bit the same: step counts, convergence, last delta_u
+    and populations."""
     geoms = domains()
     runs = []
-    for wide_below in (-1, 1000, 3):
+    for wide_below in (-1, 0, 1000, 3):
         with lbmc.Batch(geoms, tau=1.0, force=(1e-6, 0.0), collision_type=lbmc.NTPOR, storage=storage,
                         block_threads=256, steps_per_launch=50, wide_below=wide_below) as b:
             res = b.run(cap, tol, check_every=50)
