@@ -277,6 +277,24 @@ constexpr int WIDE_WARPS = WIDE_THREADS / 32;
 struct RowSegment {
   int domain, y, x0;
 };
+// What the next step of a listed domain needs, prepared once per domain and
+// step (by the host when the list is built, then by the finish kernel), so
+// that no warp divides the 64-bit step counter: the shift t mod (lx, ly) and
+// the flags below.
+struct WideStep {
+  int sx, sy;
+  int flags;
+};
+constexpr int WIDE_RUNNING = 1, WIDE_SAVE = 2, WIDE_TEST = 4;
+
+__host__ __device__ inline WideStep wide_step(long long t, int lx, int ly, int check, bool running) {
+  WideStep w;
+  w.sx = (int)(t % lx);
+  w.sy = (int)(t % ly);
+  const bool save = (t % check) == 0;
+  w.flags = (running ? WIDE_RUNNING : 0) | (save ? WIDE_SAVE : 0) | (save && t >= check ? WIDE_TEST : 0);
+  return w;
+}
 
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
@@ -286,12 +304,12 @@ __device__ __forceinline__ float warp_max(float v) {
 
 template <class S, bool BLEND>
 __global__ void __launch_bounds__(WIDE_THREADS)
-    batch_wide_kernel(const BatchArgs A, const RowSegment *segs, int nsegs, int *acc) {
+    batch_wide_kernel(const BatchArgs A, const RowSegment *segs, int nsegs, const WideStep *steps, int *acc) {
   const int si = blockIdx.x * WIDE_WARPS + (int)(threadIdx.x >> 5);
   if (si >= nsegs) return;  // whole warps
   const RowSegment G = segs[si];
-  const BatchStateDev &st = A.state[G.domain];
-  if (st.converged) return;  // warp-uniform: one domain per segment
+  const WideStep W = steps[G.domain];
+  if (!(W.flags & WIDE_RUNNING)) return;  // warp-uniform: one domain per segment
   S *pool = reinterpret_cast<S *>(A.pool);
   StepArgs<float> a;
   memset(&a, 0, sizeof(a));
@@ -302,10 +320,9 @@ __global__ void __launch_bounds__(WIDE_THREADS)
   a.scale = A.scale;
   a.inv_scale = A.inv_scale;
   const BatchDomainDev D = A.dom[G.domain];
-  const long long t = st.t;
-  const int sx = (int)(t % D.lx), sy = (int)(t % D.ly);
-  const bool save = (t % A.check) == 0;
-  const bool test = save && t >= A.check;
+  const int sx = W.sx, sy = W.sy;
+  const bool save = W.flags & WIDE_SAVE;
+  const bool test = W.flags & WIDE_TEST;
   a.B = A.B + D.node_off;
   const int x = G.x0 + (int)(threadIdx.x & 31);
   float dmax = 0;
@@ -327,14 +344,15 @@ __global__ void __launch_bounds__(WIDE_THREADS)
 // After each tail-phase step: per domain, the convergence test of the step
 // just taken (max |u(t) - u(t - C)| < tol), t + 1, the step cap; at the last
 // step of a launch group the domains still running are counted.
-__global__ void batch_wide_finish_kernel(const BatchArgs A, const int *wide, int nwide, int *acc, int last) {
+__global__ void batch_wide_finish_kernel(const BatchArgs A, const int *wide, int nwide, WideStep *steps, int *acc,
+                                         int last) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nwide) return;
   const int d = wide[i];
   BatchStateDev &st = A.state[d];
   if (st.converged) return;
   long long t = st.t;
-  const bool test = (t % A.check) == 0 && t >= A.check;
+  const bool test = steps[d].flags & WIDE_TEST;
   int stop = 0;
   if (test) {
     const float m = __int_as_float(acc[d]);
@@ -345,6 +363,8 @@ __global__ void batch_wide_finish_kernel(const BatchArgs A, const int *wide, int
   t += 1;
   if (!stop && t >= A.max_steps) stop = STOP_CAP;
   st.t = t;
+  const BatchDomainDev D = A.dom[d];
+  steps[d] = wide_step(t, D.lx, D.ly, A.check, !stop);
   if (stop) {
     st.converged = stop;
     st.done_ns = global_ns();
@@ -479,12 +499,15 @@ cudaError_t enqueue(lbmc_batch *b, int steps, int check, double tol, long long m
 struct WideWork {
   RowSegment *segs = nullptr;
   int *wide = nullptr;
+  WideStep *steps = nullptr;  // per domain (every domain, listed or not)
   int nsegs = 0, nwide = 0;
   void release() {
     if (segs) cudaFree(segs);
     if (wide) cudaFree(wide);
+    if (steps) cudaFree(steps);
     segs = nullptr;
     wide = nullptr;
+    steps = nullptr;
     nsegs = nwide = 0;
   }
 };
@@ -502,9 +525,9 @@ cudaError_t launch_wide(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hb
   auto kw = b->blend ? batch_wide_kernel<S, true> : batch_wide_kernel<S, false>;
   const unsigned grid = (unsigned)((w.nsegs + WIDE_WARPS - 1) / WIDE_WARPS);
   for (int s = 0; s < hbm.steps; s++) {
-    if (grid > 0) kw<<<grid, WIDE_THREADS, 0, b->side>>>(hbm, w.segs, w.nsegs, b->acc);
+    if (grid > 0) kw<<<grid, WIDE_THREADS, 0, b->side>>>(hbm, w.segs, w.nsegs, w.steps, b->acc);
     if (w.nwide > 0)
-      batch_wide_finish_kernel<<<(w.nwide + 127) / 128, 128, 0, b->side>>>(hbm, w.wide, w.nwide, b->acc,
+      batch_wide_finish_kernel<<<(w.nwide + 127) / 128, 128, 0, b->side>>>(hbm, w.wide, w.nwide, w.steps, b->acc,
                                                                         s == hbm.steps - 1);
   }
   e = cudaGetLastError();
@@ -528,16 +551,18 @@ cudaError_t enqueue_wide(lbmc_batch *b, int steps, int check, double tol, long l
 
 // The HBM domains still running, as row segments; device arrays in w (the
 // caller releases them).
-cudaError_t build_wide(lbmc_batch *b, WideWork &w) {
+cudaError_t build_wide(lbmc_batch *b, int check, WideWork &w) {
   std::vector<BatchStateDev> st(b->ndomains);
   cudaError_t e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return e;
   std::vector<RowSegment> segs;
   std::vector<int> wide;
+  std::vector<WideStep> steps(b->ndomains, WideStep{0, 0, 0});
   for (int d : b->order) {
     const BatchDomainDev &D = b->dom[d];
     if (D.resident || st[d].converged) continue;
     wide.push_back(d);
+    steps[d] = wide_step(st[d].t, D.lx, D.ly, check, true);
     for (int y = 0; y < D.ly; y++)
       for (int x0 = 0; x0 < D.lx; x0 += 32) segs.push_back({d, y, x0});
   }
@@ -545,6 +570,9 @@ cudaError_t build_wide(lbmc_batch *b, WideWork &w) {
   w.nwide = (int)wide.size();
   e = cudaMalloc(&w.segs, sizeof(RowSegment) * std::max(1, w.nsegs));
   if (e == cudaSuccess) e = cudaMalloc(&w.wide, sizeof(int) * std::max(1, w.nwide));
+  if (e == cudaSuccess) e = cudaMalloc(&w.steps, sizeof(WideStep) * b->ndomains);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(w.steps, steps.data(), sizeof(WideStep) * b->ndomains, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && w.nsegs)
     e = cudaMemcpy(w.segs, segs.data(), sizeof(RowSegment) * w.nsegs, cudaMemcpyHostToDevice);
   if (e == cudaSuccess && w.nwide) e = cudaMemcpy(w.wide, wide.data(), sizeof(int) * w.nwide, cudaMemcpyHostToDevice);
@@ -697,7 +725,7 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
     long long hbm_active = 0;
     for (int d = 0; d < b->ndomains; d++) hbm_active += !b->dom[d].resident && !st[d].converged;
     if (hbm_active > 0 && hbm_active < b->wide_below) {
-      e = build_wide(b, w);
+      e = build_wide(b, check_every, w);
       if (e != cudaSuccess) {
         w.release();
         return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
@@ -771,7 +799,7 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
   auto go_wide = [&]() -> cudaError_t {
     drop_graph();
     w.release();
-    cudaError_t ew = build_wide(b, w);
+    cudaError_t ew = build_wide(b, check_every, w);
     wide = ew == cudaSuccess;
     if (ew == cudaSuccess) ew = capture(graph, exec);
     return ew;
