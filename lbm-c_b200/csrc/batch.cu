@@ -264,18 +264,18 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
 __global__ void stamp_kernel(unsigned long long *out) { *out = global_ns(); }
 
 // Wide phase: one step of the listed HBM domains per launch over every SM.
-// The work is cut into row segments of 32 nodes (domain, row y, first x),
-// one per warp, two warps per block, one block per two segments: x is the
-// lane's offset in the segment and y is uniform, so no node index is
-// divided, and the row offsets of the shift layout are warp-uniform.  A
-// row whose length is not a multiple of 32 leaves lanes of its last segment
-// idle.  The convergence test's warp maxima go to acc[domain] (non-negative
+// The work is cut into segments of 32 consecutive nodes of a domain (node
+// index k = x + lx y), one per warp, two warps per block, one block per two
+// segments.  A segment records the (x, y) of its first node; a lane adds
+// its offset to x and wraps into the next row when x passes lx, so no node
+// index is divided, and only the last segment of a domain has idle lanes.
+// The convergence test's warp maxima go to acc[domain] (non-negative
 // floats compare as their bit patterns, and the positive NaN of a
 // non-finite velocity is above every one of them).
 constexpr int WIDE_THREADS = 64;
 constexpr int WIDE_WARPS = WIDE_THREADS / 32;
 struct RowSegment {
-  int domain, y, x0;
+  int domain, y, x0;  // first node (x0, y) of the segment
 };
 // What the next step of a listed domain needs, prepared once per domain and
 // step (by the host when the list is built, then by the finish kernel), so
@@ -324,13 +324,18 @@ __global__ void __launch_bounds__(WIDE_THREADS)
   const bool save = W.flags & WIDE_SAVE;
   const bool test = W.flags & WIDE_TEST;
   a.B = A.B + D.node_off;
-  const int x = G.x0 + (int)(threadIdx.x & 31);
+  const int lane = (int)(threadIdx.x & 31);
+  int x = G.x0 + lane, y = G.y;
+  while (x >= D.lx) {  // at most once when lx >= 32
+    x -= D.lx;
+    y += 1;
+  }
   float dmax = 0;
-  if (x < D.lx) {
-    const int k = x + G.y * D.lx;
+  if (y < D.ly) {
+    const int k = x + y * D.lx;
     float2 *up = A.u_prev + D.node_off;
     float ux, uy;
-    batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, G.y, D.lx, D.ly, sx, sy, A.cls[D.node_off + k], a,
+    batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, y, D.lx, D.ly, sx, sy, A.cls[D.node_off + k], a,
                          ux, uy);
     if (test) dmax = node_delta(ux, uy, up[k]);
     if (save) up[k] = make_float2(ux, uy);
@@ -563,8 +568,8 @@ cudaError_t build_wide(lbmc_batch *b, int check, WideWork &w) {
     if (D.resident || st[d].converged) continue;
     wide.push_back(d);
     steps[d] = wide_step(st[d].t, D.lx, D.ly, check, true);
-    for (int y = 0; y < D.ly; y++)
-      for (int x0 = 0; x0 < D.lx; x0 += 32) segs.push_back({d, y, x0});
+    const long long n = (long long)D.lx * D.ly;
+    for (long long k0 = 0; k0 < n; k0 += 32) segs.push_back({d, (int)(k0 / D.lx), (int)(k0 % D.lx)});
   }
   w.nsegs = (int)segs.size();
   w.nwide = (int)wide.size();
