@@ -78,6 +78,7 @@ struct BatchArgs {
   long long max_steps;
   float tau, force[2];
   float omega;               // 1/tau
+  float guo_a[9], guo_b[9], guo_odd[9];  // uniform-force Guo terms (StepArgs)
   float scale, inv_scale;
   int blend;
   size_t smem_elems;         // capacity of the shared-memory population buffer
@@ -173,6 +174,11 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
   memset(&a, 0, sizeof(a));
   a.tau = A.tau;
   a.omega = A.omega;
+  for (int i = 0; i < 9; i++) {
+    a.guo_a[i] = A.guo_a[i];
+    a.guo_b[i] = A.guo_b[i];
+    a.guo_odd[i] = A.guo_odd[i];
+  }
   a.force_u[0] = A.force[0];
   a.force_u[1] = A.force[1];
   a.scale = A.scale;
@@ -264,16 +270,19 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
 __global__ void stamp_kernel(unsigned long long *out) { *out = global_ns(); }
 
 // Wide phase: one step of the listed HBM domains per launch over every SM.
-// The work is cut into segments of 32 consecutive nodes of a domain (node
-// index k = x + lx y), one per warp, two warps per block, one block per two
-// segments.  A segment records the (x, y) of its first node; a lane adds
-// its offset to x and wraps into the next row when x passes lx, so no node
-// index is divided, and only the last segment of a domain has idle lanes.
+// The work is cut into segments of WIDE_ITERS x 32 consecutive nodes of a
+// domain (node index k = x + lx y), one per warp, two warps per block, one
+// block per two segments; a warp loads a segment's descriptors once and
+// steps 32 nodes per iteration.  A segment records the (x, y) of its first
+// node; a lane adds its offset to x and wraps into the next row when x
+// passes lx, so no node index is divided, and only the last segment of a
+// domain has idle lanes.
 // The convergence test's warp maxima go to acc[domain] (non-negative
 // floats compare as their bit patterns, and the positive NaN of a
 // non-finite velocity is above every one of them).
 constexpr int WIDE_THREADS = 64;
 constexpr int WIDE_WARPS = WIDE_THREADS / 32;
+constexpr int WIDE_ITERS = 1;  // a segment is WIDE_ITERS x 32 consecutive nodes, one warp's work
 struct RowSegment {
   int domain, y, x0;  // first node (x0, y) of the segment
 };
@@ -303,7 +312,7 @@ __device__ __forceinline__ float warp_max(float v) {
 }
 
 template <class S, bool BLEND>
-__global__ void __launch_bounds__(WIDE_THREADS)
+__global__ void __launch_bounds__(WIDE_THREADS, 20)
     batch_wide_kernel(const BatchArgs A, const RowSegment *segs, int nsegs, const WideStep *steps, int *acc) {
   const int si = blockIdx.x * WIDE_WARPS + (int)(threadIdx.x >> 5);
   if (si >= nsegs) return;  // whole warps
@@ -315,6 +324,11 @@ __global__ void __launch_bounds__(WIDE_THREADS)
   memset(&a, 0, sizeof(a));
   a.tau = A.tau;
   a.omega = A.omega;
+  for (int i = 0; i < 9; i++) {
+    a.guo_a[i] = A.guo_a[i];
+    a.guo_b[i] = A.guo_b[i];
+    a.guo_odd[i] = A.guo_odd[i];
+  }
   a.force_u[0] = A.force[0];
   a.force_u[1] = A.force[1];
   a.scale = A.scale;
@@ -331,14 +345,20 @@ __global__ void __launch_bounds__(WIDE_THREADS)
     y += 1;
   }
   float dmax = 0;
-  if (y < D.ly) {
+  float2 *up = A.u_prev + D.node_off;
+  for (int j = 0; j < WIDE_ITERS; j++) {
+    if (y >= D.ly) break;  // past the domain's last node
     const int k = x + y * D.lx;
-    float2 *up = A.u_prev + D.node_off;
     float ux, uy;
     batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, y, D.lx, D.ly, sx, sy, A.cls[D.node_off + k], a,
                          ux, uy);
-    if (test) dmax = node_delta(ux, uy, up[k]);
+    if (test) dmax = nan_max(dmax, node_delta(ux, uy, up[k]));
     if (save) up[k] = make_float2(ux, uy);
+    x += 32;
+    while (x >= D.lx) {
+      x -= D.lx;
+      y += 1;
+    }
   }
   if (test) {
     const float m = warp_max(dmax);
@@ -477,6 +497,15 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
   A.max_steps = max_steps;
   A.tau = (float)b->cfg.tau;
   A.omega = (float)(1.0 / b->cfg.tau);
+  {
+    float ga[15], gb[15], go[15];
+    set_uniform_guo<D2Q9, float>(ga, gb, go, b->cfg.tau, b->cfg.force);
+    for (int i = 0; i < 9; i++) {
+      A.guo_a[i] = ga[i];
+      A.guo_b[i] = gb[i];
+      A.guo_odd[i] = go[i];
+    }
+  }
   A.force[0] = (float)b->cfg.force[0];
   A.force[1] = (float)b->cfg.force[1];
   A.scale = (float)b->scale;
@@ -569,7 +598,7 @@ cudaError_t build_wide(lbmc_batch *b, int check, WideWork &w) {
     wide.push_back(d);
     steps[d] = wide_step(st[d].t, D.lx, D.ly, check, true);
     const long long n = (long long)D.lx * D.ly;
-    for (long long k0 = 0; k0 < n; k0 += 32) segs.push_back({d, (int)(k0 / D.lx), (int)(k0 % D.lx)});
+    for (long long k0 = 0; k0 < n; k0 += 32 * WIDE_ITERS) segs.push_back({d, (int)(k0 / D.lx), (int)(k0 % D.lx)});
   }
   w.nsegs = (int)segs.size();
   w.nwide = (int)wide.size();

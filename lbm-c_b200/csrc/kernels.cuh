@@ -293,6 +293,10 @@ struct StepArgs {
   int n;
   C tau;
   C omega;    // 1/tau
+  // Guo source terms of a uniform force F (force[] all null), per population
+  // i, with pre = 1 - 1/(2 tau): guo_a = 9 w_i pre (e_i.F), guo_b = 3 w_i pre,
+  // guo_odd = 3 w_i pre (e_i.F); the even part is guo_a (e_i.u) - guo_b (u.F).
+  C guo_a[15], guo_b[15], guo_odd[15];
   C s_mrt[15];
   C c_smag;
   C scale, inv_scale;
@@ -309,6 +313,22 @@ struct StepArgs {
 };
 
 constexpr unsigned ERROR_TIMEOUT = 1u;
+
+// Fills the uniform-force Guo terms of StepArgs (host side).
+template <class L, class C>
+void set_uniform_guo(C (&ga)[15], C (&gb)[15], C (&godd)[15], double tau, const double *force) {
+  const double pre = 1.0 - 1.0 / (2.0 * tau);
+  for (int i = 0; i < 15; i++) {
+    ga[i] = gb[i] = godd[i] = C(0);
+    if (i >= L::Q) continue;
+    double eF = 0;
+    for (int d = 0; d < L::DIM; d++) eF += L::e(d, i) * force[d];
+    const double w = (double)L::wn(i) / (double)L::wd;
+    ga[i] = (C)(9.0 * w * pre * eF);
+    gb[i] = (C)(3.0 * w * pre);
+    godd[i] = (C)(3.0 * w * pre * eF);
+  }
+}
 
 // ----------------------------------------------------------- index helpers
 
@@ -857,7 +877,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
     nd.u[0] += h * F[0];
     nd.u[1] += h * F[1];
     if (L::DIM > 2) nd.u[2] += h * F[2];
-    pre = C(1) - recip(C(2) * tau0);
+    if (a.force[0]) pre = C(1) - recip(C(2) * tau0);
     uF = nd.u[0] * F[0] + nd.u[1] * F[1] + (L::DIM > 2 ? nd.u[2] * F[2] : C(0));
   }
   const C omb = C(1) - B;
@@ -866,10 +886,16 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
   auto guo_parts = [&](auto ic, C &even, C &odd) {
     if constexpr (FORCE) {
       constexpr int i = decltype(ic)::value;
-      const C wp = C(weight<L>(i)) * pre;
-      const C eF = edot<L, i>(F), eu = edot<L, i>(nd.u);
-      even = wp * (C(9) * eu * eF - C(3) * uF);
-      odd = wp * C(3) * eF;
+      const C eu = edot<L, i>(nd.u);
+      if (!a.force[0]) {  // uniform force: the host's per-population terms
+        even = a.guo_a[i] * eu - a.guo_b[i] * uF;
+        odd = a.guo_odd[i];
+      } else {
+        const C wp = C(weight<L>(i)) * pre;
+        const C eF = edot<L, i>(F);
+        even = wp * (C(9) * eu * eF - C(3) * uF);
+        odd = wp * C(3) * eF;
+      }
     } else {
       even = 0;
       odd = 0;
