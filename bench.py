@@ -279,7 +279,8 @@ def run_batch(args, world, rank, local):
 
     def batched(storage, cap):
         torch.cuda.synchronize(dev)
-        b = lbmc.Batch(geoms, tau=tau, force=(g, 0.0), storage=storage, wide_below=args.wide_below)
+        b = lbmc.Batch(geoms, tau=tau, force=(g, 0.0), storage=storage, wide_below=args.wide_below,
+                       wide_min_nodes=args.wide_min_nodes)
         t1 = time.perf_counter()
         res = b.run(cap, tol, check)
         torch.cuda.synchronize(dev)
@@ -724,9 +725,12 @@ def main():
     ap.add_argument("--workload", choices=list(WORKLOAD_METRIC), default="porous")
     ap.add_argument("--domains", type=int, default=4096)
     ap.add_argument("--batch-cap", type=int, default=20000)
+    ap.add_argument("--wide-min-nodes", type=int, default=0,
+                    help="batched sweep: HBM domains of at least this many nodes are stepped over "
+                         "every SM, the others one block per domain (0 = the storage's default)")
     ap.add_argument("--wide-below", type=int, default=0,
-                    help="batched sweep: step the HBM domains over every SM once fewer than this "
-                         "many run (0 = from the start, -1 = never: one block per domain)")
+                    help="batched sweep: the one-block-per-domain HBM domains join the wide path "
+                         "once fewer than this many run (0 = half the SMs, -1 = never)")
     ap.add_argument("--alone-sample", type=int, default=32)
     ap.add_argument("--e2e-reps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")

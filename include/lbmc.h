@@ -260,11 +260,14 @@ typedef struct lbmc_batch_config {
   int device;
   int block_threads;    /* 0 = autotune (256/512/1024) */
   int steps_per_launch; /* 0 = autotune (check_every or 4*check_every) */
-  int wide_below;       /* domains too large for shared memory are stepped one step per launch
-                           over every SM once fewer than this many of them are running, and
-                           before that one block per domain, K steps per launch; 0 = default
-                           (over every SM from the start), < 0 = never */
-  int reserved[7];
+  int wide_min_nodes;   /* domains too large for shared memory with at least this many nodes
+                           are stepped one step per launch over every SM, the others one block
+                           per domain, K steps per launch; 0 = default (FP32: 1, every such
+                           domain; FP16/BF16: 131072) */
+  int wide_below;       /* the one-block-per-domain ones join the wide path once fewer than
+                           this many of them are running; 0 = default (half the SMs), < 0 =
+                           never */
+  int reserved[6];
 } lbmc_batch_config;
 
 typedef struct lbmc_batch_domain {

@@ -405,8 +405,12 @@ struct lbmc_batch {
   lbmc_batch_config cfg;
   int ndomains = 0;
   std::vector<BatchDomainDev> dom;
-  std::vector<int> order;      // resident domains, then HBM domains, each largest first
-  int n_resident = 0;
+  // Domain classes, each largest first: resident (shared memory), then
+  // block-stepped HBM domains (one block per domain, K steps per launch),
+  // then wide HBM domains (over every SM, one step per launch).
+  std::vector<int> order;
+  int n_resident = 0, n_block = 0;
+  long long wide_min_nodes = 0;  // HBM domains with at least this many nodes are wide
   void *pool = nullptr;
   uint8_t *cls = nullptr;
   float *B = nullptr;
@@ -414,9 +418,10 @@ struct lbmc_batch {
   BatchDomainDev *dom_dev = nullptr;
   BatchStateDev *state = nullptr;
   int *order_dev = nullptr;
-  int *counters = nullptr;  // [0] resident queue, [1] HBM queue, [2] active, [3] active in HBM
+  int *counters = nullptr;  // [0] resident queue, [1] block-stepped queue, [2] active,
+                            // [3] active block-stepped, [4] active wide
   int *acc = nullptr;       // tail phase: per-domain convergence maxima (float bits)
-  int wide_below = 0;       // tail-phase threshold (active HBM domains)
+  int wide_below = 0;       // move the block-stepped domains to the wide path below this many
   unsigned long long *t0 = nullptr;
   cudaStream_t stream = nullptr;
   int ssize = 4;
@@ -455,29 +460,9 @@ cudaError_t configure_batch(lbmc_batch *b) {
   return e;
 }
 
-template <class S>
-cudaError_t launch_batch(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hbm, int threads,
-                         cudaStream_t st) {
-  // Resident domains on st, HBM domains on the side stream, joined again.
-  cudaError_t e = cudaEventRecord(b->fork, st);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->fork, 0);
-  if (e != cudaSuccess) return e;
-  if (res.ndomains > 0) {
-    auto kr = b->blend ? batch_kernel<S, true, true> : batch_kernel<S, false, true>;
-    kr<<<b->sms, threads, b->smem_bytes, st>>>(res);
-  }
-  if (hbm.ndomains > 0) {
-    const int k = threads <= 256 ? 0 : (threads <= 512 ? 1 : 2);
-    auto kh = b->blend ? batch_kernel<S, true, false> : batch_kernel<S, false, false>;
-    kh<<<b->sms * b->hbm_blocks_per_sm[k], threads, 0, b->side>>>(hbm);
-  }
-  e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaEventRecord(b->join, b->side);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->join, 0);
-  return e;
-}
+enum DomainClass { CLASS_RESIDENT, CLASS_BLOCK, CLASS_WIDE };
 
-BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long max_steps, bool resident) {
+BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long max_steps, DomainClass c) {
   BatchArgs A;
   memset(&A, 0, sizeof(A));
   A.pool = b->pool;
@@ -486,11 +471,11 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
   A.u_prev = b->u_prev;
   A.dom = b->dom_dev;
   A.state = b->state;
-  A.order = b->order_dev + (resident ? 0 : b->n_resident);
-  A.ndomains = resident ? b->n_resident : b->ndomains - b->n_resident;
-  A.queue = b->counters + (resident ? 0 : 1);
+  A.order = b->order_dev + (c == CLASS_RESIDENT ? 0 : b->n_resident);
+  A.ndomains = c == CLASS_RESIDENT ? b->n_resident : (c == CLASS_BLOCK ? b->n_block : 0);
+  A.queue = b->counters + (c == CLASS_RESIDENT ? 0 : 1);
   A.active = b->counters + 2;
-  A.active_hbm = b->counters + 3;
+  A.active_hbm = b->counters + (c == CLASS_WIDE ? 4 : 3);
   A.steps = steps;
   A.check = check;
   A.tol = (float)tol;
@@ -511,25 +496,12 @@ BatchArgs make_args(lbmc_batch *b, int steps, int check, double tol, long long m
   A.scale = (float)b->scale;
   A.inv_scale = (float)(1.0 / b->scale);
   A.blend = b->blend;
-  A.smem_elems = resident ? b->smem_bytes / b->ssize : 0;
+  A.smem_elems = c == CLASS_RESIDENT ? b->smem_bytes / b->ssize : 0;
   return A;
 }
 
-cudaError_t enqueue(lbmc_batch *b, int steps, int check, double tol, long long max_steps, int threads,
-                    cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(b->counters, 0, 4 * sizeof(int), st);
-  if (e != cudaSuccess) return e;
-  const BatchArgs res = make_args(b, steps, check, tol, max_steps, true);
-  const BatchArgs hbm = make_args(b, steps, check, tol, max_steps, false);
-  switch (b->cfg.storage) {
-    case LBMC_F16: return launch_batch<__half>(b, res, hbm, threads, st);
-    case LBMC_BF16: return launch_batch<__nv_bfloat16>(b, res, hbm, threads, st);
-    default: return launch_batch<float>(b, res, hbm, threads, st);
-  }
-}
-
-// Tail phase: the listed HBM domains on every SM (per step: tiles, then the
-// per-domain finish), resident domains as before, in two graph branches.
+// The wide domains still running, as node segments, with their step
+// descriptors (device arrays; release() frees them).
 struct WideWork {
   RowSegment *segs = nullptr;
   int *wide = nullptr;
@@ -546,9 +518,12 @@ struct WideWork {
   }
 };
 
+// One graph launch: the resident kernel on st; on the side stream the
+// block-stepped kernel (unless its domains moved to the wide path) and then
+// K wide steps; joined again.
 template <class S>
-cudaError_t launch_wide(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hbm, int threads, const WideWork &w,
-                        cudaStream_t st) {
+cudaError_t launch_round(lbmc_batch *b, const BatchArgs &res, const BatchArgs &blk, const BatchArgs &wid,
+                         int threads, bool run_block, const WideWork &w, cudaStream_t st) {
   cudaError_t e = cudaEventRecord(b->fork, st);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->fork, 0);
   if (e != cudaSuccess) return e;
@@ -556,13 +531,19 @@ cudaError_t launch_wide(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hb
     auto kr = b->blend ? batch_kernel<S, true, true> : batch_kernel<S, false, true>;
     kr<<<b->sms, threads, b->smem_bytes, st>>>(res);
   }
-  auto kw = b->blend ? batch_wide_kernel<S, true> : batch_wide_kernel<S, false>;
-  const unsigned grid = (unsigned)((w.nsegs + WIDE_WARPS - 1) / WIDE_WARPS);
-  for (int s = 0; s < hbm.steps; s++) {
-    if (grid > 0) kw<<<grid, WIDE_THREADS, 0, b->side>>>(hbm, w.segs, w.nsegs, w.steps, b->acc);
-    if (w.nwide > 0)
-      batch_wide_finish_kernel<<<(w.nwide + 127) / 128, 128, 0, b->side>>>(hbm, w.wide, w.nwide, w.steps, b->acc,
-                                                                        s == hbm.steps - 1);
+  if (run_block && blk.ndomains > 0) {
+    const int k = threads <= 256 ? 0 : (threads <= 512 ? 1 : 2);
+    auto kh = b->blend ? batch_kernel<S, true, false> : batch_kernel<S, false, false>;
+    kh<<<b->sms * b->hbm_blocks_per_sm[k], threads, 0, b->side>>>(blk);
+  }
+  if (w.nwide > 0) {
+    auto kw = b->blend ? batch_wide_kernel<S, true> : batch_wide_kernel<S, false>;
+    const unsigned grid = (unsigned)((w.nsegs + WIDE_WARPS - 1) / WIDE_WARPS);
+    for (int s = 0; s < wid.steps; s++) {
+      kw<<<grid, WIDE_THREADS, 0, b->side>>>(wid, w.segs, w.nsegs, w.steps, b->acc);
+      batch_wide_finish_kernel<<<(w.nwide + 127) / 128, 128, 0, b->side>>>(wid, w.wide, w.nwide, w.steps, b->acc,
+                                                                          s == wid.steps - 1);
+    }
   }
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaEventRecord(b->join, b->side);
@@ -570,31 +551,34 @@ cudaError_t launch_wide(lbmc_batch *b, const BatchArgs &res, const BatchArgs &hb
   return e;
 }
 
-cudaError_t enqueue_wide(lbmc_batch *b, int steps, int check, double tol, long long max_steps, int threads,
-                         const WideWork &w, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(b->counters, 0, 4 * sizeof(int), st);
+cudaError_t enqueue_round(lbmc_batch *b, int steps, int check, double tol, long long max_steps, int threads,
+                          bool run_block, const WideWork &w, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(b->counters, 0, 5 * sizeof(int), st);
   if (e != cudaSuccess) return e;
-  const BatchArgs res = make_args(b, steps, check, tol, max_steps, true);
-  const BatchArgs hbm = make_args(b, steps, check, tol, max_steps, false);
+  const BatchArgs res = make_args(b, steps, check, tol, max_steps, CLASS_RESIDENT);
+  const BatchArgs blk = make_args(b, steps, check, tol, max_steps, CLASS_BLOCK);
+  const BatchArgs wid = make_args(b, steps, check, tol, max_steps, CLASS_WIDE);
   switch (b->cfg.storage) {
-    case LBMC_F16: return launch_wide<__half>(b, res, hbm, threads, w, st);
-    case LBMC_BF16: return launch_wide<__nv_bfloat16>(b, res, hbm, threads, w, st);
-    default: return launch_wide<float>(b, res, hbm, threads, w, st);
+    case LBMC_F16: return launch_round<__half>(b, res, blk, wid, threads, run_block, w, st);
+    case LBMC_BF16: return launch_round<__nv_bfloat16>(b, res, blk, wid, threads, run_block, w, st);
+    default: return launch_round<float>(b, res, blk, wid, threads, run_block, w, st);
   }
 }
 
-// The HBM domains still running, as row segments; device arrays in w (the
-// caller releases them).
-cudaError_t build_wide(lbmc_batch *b, int check, WideWork &w) {
+// The wide domains still running (with include_block the block-stepped ones
+// too), as node segments; device arrays in w (the caller releases them).
+cudaError_t build_wide(lbmc_batch *b, int check, bool include_block, WideWork &w) {
   std::vector<BatchStateDev> st(b->ndomains);
   cudaError_t e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return e;
   std::vector<RowSegment> segs;
   std::vector<int> wide;
   std::vector<WideStep> steps(b->ndomains, WideStep{0, 0, 0});
-  for (int d : b->order) {
+  for (int j = b->n_resident; j < b->ndomains; j++) {
+    const int d = b->order[j];
     const BatchDomainDev &D = b->dom[d];
-    if (D.resident || st[d].converged) continue;
+    const bool block_stepped = j < b->n_resident + b->n_block;
+    if (st[d].converged || (block_stepped && !include_block)) continue;
     wide.push_back(d);
     steps[d] = wide_step(st[d].t, D.lx, D.ly, check, true);
     const long long n = (long long)D.lx * D.ly;
@@ -683,13 +667,28 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
       if (c == 2) b->blend = true;
     }
   }
+  // HBM domains with at least wide_min_nodes nodes are stepped over every
+  // SM; the default per storage is the measured better choice on the
+  // 4096-domain sweep (FP32: every HBM domain wide; FP16/BF16: only those of
+  // at least 131,072 nodes, the others one block per domain, whose K steps
+  // then mostly hit in cache).
+  b->wide_min_nodes = cfg->wide_min_nodes > 0 ? cfg->wide_min_nodes
+                                              : (cfg->storage == LBMC_F32 ? 1 : (1LL << 17));
+  auto klass = [&](int d) {
+    const BatchDomainDev &D = b->dom[d];
+    if (D.resident) return 0;
+    return (long long)D.lx * D.ly >= b->wide_min_nodes ? 2 : 1;
+  };
   b->order.resize(ndomains);
   std::iota(b->order.begin(), b->order.end(), 0);
   std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
-    if (b->dom[x].resident != b->dom[y].resident) return b->dom[x].resident > b->dom[y].resident;
+    if (klass(x) != klass(y)) return klass(x) < klass(y);
     return (long long)b->dom[x].lx * b->dom[x].ly > (long long)b->dom[y].lx * b->dom[y].ly;
   });
-  for (const auto &D : b->dom) b->n_resident += D.resident;
+  for (int d = 0; d < ndomains; d++) {
+    b->n_resident += klass(d) == 0;
+    b->n_block += klass(d) == 1;
+  }
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void **p, size_t bytes) {
     if (e == cudaSuccess) e = cudaMalloc(p, bytes ? bytes : 16);
@@ -701,7 +700,7 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   alloc((void **)&b->dom_dev, ndomains * sizeof(BatchDomainDev));
   alloc((void **)&b->state, ndomains * sizeof(BatchStateDev));
   alloc((void **)&b->order_dev, ndomains * sizeof(int));
-  alloc((void **)&b->counters, 4 * sizeof(int));
+  alloc((void **)&b->counters, 5 * sizeof(int));
   alloc((void **)&b->acc, ndomains * sizeof(int));
   alloc((void **)&b->t0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(b->pool, 0, (size_t)pop * b->ssize);  // f = w (Init 0)
@@ -735,7 +734,7 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
   }
   b->threads = cfg->block_threads;
   b->steps = cfg->steps_per_launch;
-  b->wide_below = cfg->wide_below == 0 ? INT_MAX : cfg->wide_below;
+  b->wide_below = cfg->wide_below == 0 ? b->sms / 2 : cfg->wide_below;
   *out = b;
   return LBMC_OK;
 }
@@ -748,28 +747,25 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
   cudaError_t e = cudaSuccess;
   stamp_kernel<<<1, 1, 0, b->stream>>>(b->t0);
 
-  // The wide phase (HBM domains stepped over every SM) starts once fewer
-  // than wide_below HBM domains are running: at once with the default.
+  // Wide domains run over every SM from the start; the block-stepped ones
+  // join them once fewer than wide_below of those are running.
   WideWork w;
-  bool wide = false;
-  if (b->wide_below > 0) {
+  bool all_wide = false;  // the block-stepped domains moved to the wide path
+  {
     std::vector<BatchStateDev> st(b->ndomains);
     e = cudaMemcpy(st.data(), b->state, b->ndomains * sizeof(BatchStateDev), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
-    long long hbm_active = 0;
-    for (int d = 0; d < b->ndomains; d++) hbm_active += !b->dom[d].resident && !st[d].converged;
-    if (hbm_active > 0 && hbm_active < b->wide_below) {
-      e = build_wide(b, check_every, w);
-      if (e != cudaSuccess) {
-        w.release();
-        return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
-      }
-      wide = true;
+    long long block_active = 0;
+    for (int j = b->n_resident; j < b->n_resident + b->n_block; j++) block_active += !st[b->order[j]].converged;
+    all_wide = b->wide_below > 0 && block_active > 0 && block_active < b->wide_below;
+    e = build_wide(b, check_every, all_wide, w);
+    if (e != cudaSuccess) {
+      w.release();
+      return berr(LBMC_ERR_CUDA, std::string("lbmc_batch_run: ") + cudaGetErrorString(e));
     }
   }
   auto enqueue_any = [&](int steps, int threads) {
-    return wide ? enqueue_wide(b, steps, check_every, tol, max_steps, threads, w, b->stream)
-                : enqueue(b, steps, check_every, tol, max_steps, threads, b->stream);
+    return enqueue_round(b, steps, check_every, tol, max_steps, threads, !all_wide, w, b->stream);
   };
 
   // Autotune the launch shape on the first launches (they are real steps).
@@ -810,9 +806,9 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
   }
 
   // Capture one launch (queue reset + the kernels of K steps) in a graph and
-  // replay it.  In the wide phase the graph holds the row segments of the
-  // HBM domains still running; once a quarter of them have stopped, the
-  // segments are rebuilt so that launches no longer visit stopped domains.
+  // replay it.  Once a quarter of the listed wide domains have stopped, their
+  // segments are rebuilt and the graph re-captured, so launches no longer
+  // visit them; the same when the block-stepped domains join the wide path.
   auto capture = [&](cudaGraph_t &graph, cudaGraphExec_t &exec) -> cudaError_t {
     cudaError_t ec = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (ec != cudaSuccess) return ec;
@@ -830,24 +826,27 @@ extern "C" lbmc_status lbmc_batch_run(lbmc_batch *b, long long max_steps, double
     exec = nullptr;
     graph = nullptr;
   };
-  auto go_wide = [&]() -> cudaError_t {
+  auto rebuild = [&]() -> cudaError_t {
     drop_graph();
     w.release();
-    cudaError_t ew = build_wide(b, check_every, w);
-    wide = ew == cudaSuccess;
+    cudaError_t ew = build_wide(b, check_every, all_wide, w);
     if (ew == cudaSuccess) ew = capture(graph, exec);
     return ew;
   };
   if (e == cudaSuccess) e = capture(graph, exec);
-  int counts[4] = {0, 0, 1, 0};
+  int counts[5] = {0, 0, 1, 0, 0};
   const long long launches_max = max_steps / std::max(1, b->steps) + 2;
   for (long long l = 0; e == cudaSuccess && counts[2] > 0 && l < launches_max; l++) {
     e = cudaGraphLaunch(exec, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(counts, b->counters, sizeof(counts), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess || counts[2] == 0) break;
-    if (!wide && b->wide_below > 0 && counts[3] > 0 && counts[3] < b->wide_below) e = go_wide();
-    else if (wide && counts[3] > 0 && 4LL * counts[3] < 3LL * w.nwide) e = go_wide();
+    if (!all_wide && b->wide_below > 0 && counts[3] > 0 && counts[3] < b->wide_below) {
+      all_wide = true;
+      e = rebuild();
+    } else if (w.nwide > 0 && 4LL * counts[4] < 3LL * w.nwide) {
+      e = rebuild();
+    }
   }
   drop_graph();
   w.release();

@@ -332,7 +332,8 @@ class BatchConfig(ctypes.Structure):
                 ("collision_type", ctypes.c_int), ("storage", ctypes.c_int),
                 ("storage_scale", ctypes.c_double), ("device", ctypes.c_int),
                 ("block_threads", ctypes.c_int), ("steps_per_launch", ctypes.c_int),
-                ("wide_below", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+                ("wide_min_nodes", ctypes.c_int), ("wide_below", ctypes.c_int),
+                ("reserved", ctypes.c_int * 6)]
 
 
 class BatchDomain(ctypes.Structure):
@@ -370,7 +371,7 @@ class Batch:
 
     def __init__(self, geometries, tau=1.0, force=(1e-6, 0.0), collision_type=NTPOR,
                  storage=F16, storage_scale=0.0, device=0, block_threads=0, steps_per_launch=0,
-                 wide_below=0):
+                 wide_below=0, wide_min_nodes=0):
         lib = _batch_lib()
         cfg = BatchConfig()
         cfg.tau = tau
@@ -382,6 +383,7 @@ class Batch:
         cfg.block_threads = block_threads
         cfg.steps_per_launch = steps_per_launch
         cfg.wide_below = wide_below
+        cfg.wide_min_nodes = wide_min_nodes
         self._keep = []
         doms = (BatchDomain * len(geometries))()
         self.shapes = []

@@ -72,18 +72,20 @@ def test_batch_converges_and_freezes(lbmc):
 # tolerance above it lets its domains converge too.
 @pytest.mark.parametrize("storage,tol,cap", [("f32", 1e-9, 200000), ("f16", 1e-5, 50000)])
 def test_batch_tail_phase_is_bit_identical(lbmc, storage, tol, cap):
-    """The wide phase (HBM domains spread over every SM, one step per launch,
-    row segments rebuilt as domains stop) and the one-domain-per-block phase
-    run the same node update and the same convergence rule, so a batch run to
-    steady state never in the wide phase, wholly in it (the default, and an
-    explicit threshold), or switching to it once fewer than 3 HBM domains are
-    left, ends bit for bit the same: step counts, convergence, last delta_u
-    and populations."""
+    """The wide path (HBM domains spread over every SM, one step per launch,
+    segments rebuilt as domains stop) and the one-block-per-domain path run
+    the same node update and the same convergence rule, so a batch run to
+    steady state ends bit for bit the same (step counts, convergence, last
+    delta_u and populations) whichever path each HBM domain takes: all one
+    block per domain, all wide, split by size (12000 nodes: two of the four
+    HBM domains each way), the storage's default split, and block-stepped
+    domains that join the wide path once fewer than 3 of them are left."""
     geoms = domains()
     runs = []
-    for wide_below in (-1, 0, 1000, 3):
+    for wide_min, wide_below in ((1 << 30, -1), (1, -1), (12000, -1), (0, 0), (1 << 30, 3)):
         with lbmc.Batch(geoms, tau=1.0, force=(1e-6, 0.0), collision_type=lbmc.NTPOR, storage=storage,
-                        block_threads=256, steps_per_launch=50, wide_below=wide_below) as b:
+                        block_threads=256, steps_per_launch=50, wide_below=wide_below,
+                        wide_min_nodes=wide_min) as b:
             res = b.run(cap, tol, check_every=50)
             runs.append(([(r.steps, r.converged, r.delta_u) for r in res],
                          [b.fetch(d, lbmc.FIELD_F) for d in range(len(geoms))]))
@@ -96,18 +98,20 @@ def test_batch_tail_phase_is_bit_identical(lbmc, storage, tol, cap):
 
 
 @pytest.mark.parametrize("storage,wide_below", [("f32", -1), ("f32", 100), ("f16", -1)])
-def test_batch_nonfinite_domain_is_reported(lbmc, storage, wide_below):
+@pytest.mark.parametrize("wide_min", [1 << 30, 1])
+def test_batch_nonfinite_domain_is_reported(lbmc, storage, wide_below, wide_min):
     """A domain whose velocity turns non-finite is stopped and flagged, not
     taken for converged (a max that drops NaN would read it as Delta u = 0).
     The planted fault is on the host: a negative porosity patch in one
     domain kept in shared memory and one stepped in HBM, which the
     Noble-Torczynski blend amplifies until the populations overflow.
-    wide_below = 100 puts the HBM domains in the tail phase from the start."""
+    wide_below = 100 moves the block-stepped HBM domains to the wide path at
+    once; wide_min = 1 puts every HBM domain there from the start."""
     geoms = [g.copy() for g in domains(seed=9)[:4]]
     for d in (1, 3):
         geoms[d][2:6, 2:6] = -50.0
     with lbmc.Batch(geoms, tau=1.0, force=(1e-6, 0.0), storage=storage,
-                    wide_below=wide_below) as b:
+                    wide_below=wide_below, wide_min_nodes=wide_min) as b:
         if storage == "f32":  # FP16 rows are half as long: all four fit in shared memory
             assert b.info()["resident_domains"] == 2
         with pytest.raises(lbmc.LbmcError) as ei:
