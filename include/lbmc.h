@@ -262,8 +262,8 @@ typedef struct lbmc_batch_config {
   int steps_per_launch; /* 0 = autotune (check_every or 4*check_every) */
   int wide_min_nodes;   /* domains too large for shared memory with at least this many nodes
                            are stepped one step per launch over every SM, the others one block
-                           per domain, K steps per launch; 0 = default (FP32: 1, every such
-                           domain; FP16/BF16: 131072) */
+                           per domain, K steps per launch; 0 = default (FP32: 32768;
+                           FP16/BF16: none) */
   int wide_below;       /* the one-block-per-domain ones join the wide path once fewer than
                            this many of them are running; 0 = default (half the SMs), < 0 =
                            never */

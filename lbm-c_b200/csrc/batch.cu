@@ -7,26 +7,27 @@
 // memory are stepped by one persistent kernel: blocks take whole domains
 // from an atomic queue (largest first), load one, step it K times in shared
 // memory (the step-to-step dependency is a __syncthreads) and write it back,
-// so K steps cost one read and one write of HBM.  Domains too large for
-// shared memory are stepped in HBM one step per launch over every SM
-// (batch_wide_kernel: one warp per 32-node row segment, all running HBM
-// domains in one launch), followed by a one-thread-per-domain kernel
-// (batch_wide_finish_kernel) for the convergence test and step accounting;
-// K such step pairs run in a second branch of the same CUDA graph.  Every C
+// so K steps cost one read and one write of HBM.  Larger domains are
+// stepped in HBM in one of two ways, by size (wide_min_nodes):
+//   - one block per domain, K steps per launch (the same persistent kernel
+//     without the shared-memory copy): a domain's K steps run back to back,
+//     so a 2-byte domain of moderate size is re-read from cache;
+//   - over every SM, one step per launch (batch_wide_kernel: one warp per
+//     segment of consecutive nodes, every listed domain in one launch),
+//     followed by a one-thread-per-domain kernel (batch_wide_finish_kernel)
+//     for the convergence test and step accounting.  Large domains need the
+//     most steps and would otherwise finish last on one SM each.
+// One CUDA graph launch holds the shared-memory kernel in one branch and the
+// block-stepped kernel followed by K wide step pairs in the other.  Every C
 // steps a domain compares u with its value C steps earlier (max norm) and
 // freezes once below the tolerance, recording the device timer.  The host
 // replays the graph until every domain converged, stopped or hit the step
-// cap; once a quarter of the listed HBM domains have stopped, their row
-// segments are rebuilt and the graph re-captured, so launches stop visiting
-// them.  An autotuner times the first launches with several block sizes for
-// the shared-memory kernel and two values of K, and keeps the fastest.
-//
-// The HBM domains can also run in the persistent kernel, one block per
-// domain, K steps per launch (lbmc_batch_config.wide_below < 0, or until
-// fewer than wide_below remain): that design leaves SMs idle when few large
-// domains are running (measured: 64 domains of 512 x 512 at 11 GLUPS against
-// 53 GLUPS over every SM).  The same node update runs in both kernels, so
-// results do not depend on where a step ran.
+// cap.  Once fewer than wide_below block-stepped domains run, they join the
+// wide path; whenever a quarter of the listed wide domains have stopped,
+// the segments are rebuilt and the graph re-captured, so launches stop
+// visiting them.  An autotuner times the first launches with several block
+// sizes and two values of K, and keeps the fastest.  The same node update
+// runs in every kernel, so results do not depend on where a step ran.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -668,12 +669,14 @@ extern "C" lbmc_status lbmc_batch_init(const lbmc_batch_config *cfg, int ndomain
     }
   }
   // HBM domains with at least wide_min_nodes nodes are stepped over every
-  // SM; the default per storage is the measured better choice on the
-  // 4096-domain sweep (FP32: every HBM domain wide; FP16/BF16: only those of
-  // at least 131,072 nodes, the others one block per domain, whose K steps
-  // then mostly hit in cache).
+  // SM from the start.  Defaults measured on the 4096-domain sweep (first
+  // 20000 steps, aggregate GLUPS for thresholds 1 / 32768 / 65536 / 131072 /
+  // none): FP32 52.3 / 55.4 / 54.1 / 52.0 / 50.3, FP16 66.1 / 71.2 / 74.7 /
+  // 78.2 / 80.2 (2-byte domains stepped K times by one block stay in cache).
+  // Either way the last block-stepped domains join the wide path
+  // (wide_below), which shortens the time to steady state.
   b->wide_min_nodes = cfg->wide_min_nodes > 0 ? cfg->wide_min_nodes
-                                              : (cfg->storage == LBMC_F32 ? 1 : (1LL << 17));
+                                              : (cfg->storage == LBMC_F32 ? 32768 : LLONG_MAX);
   auto klass = [&](int d) {
     const BatchDomainDev &D = b->dom[d];
     if (D.resident) return 0;
