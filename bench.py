@@ -106,27 +106,31 @@ class ClockSampler:
         except Exception:
             return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
-    def _poll(self):
+    def _sample(self):
         nv, h = self.nvml
         bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
-        max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((float(mhz), float(self.max_mhz), {k for k, b in bits.items() if r & b}))
+        except Exception:
+            pass
+
+    def _poll(self):
         while not self.stop.is_set():
-            try:
-                mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append((float(mhz), float(max_mhz),
-                                     {k for k, b in bits.items() if r & b}))
-            except Exception:
-                pass
+            self._sample()
             self.stop.wait(self.period)
 
     def __enter__(self):
         try:
             self.nvml = self._nvml_handle()
+            nv, h = self.nvml
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
             self.source = "nvml 2 ms"
+            self._sample()  # one sample at the start, however short the region
             self.thread = threading.Thread(target=self._poll, daemon=True)
             self.thread.start()
             return self
@@ -159,6 +163,7 @@ class ClockSampler:
         self.stop.set()
         if self.nvml is not None:
             self.thread.join(timeout=5)
+            self._sample()  # and one at the end
         if self.proc is not None:
             self.proc.terminate()
             try:
