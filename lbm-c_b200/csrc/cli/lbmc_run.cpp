@@ -3,7 +3,7 @@
 // input file, builds the model from the domain directory, runs the time
 // loop with file output, screen messages and the steady-state test, and
 // exits with 1 when the state becomes non-finite, as the reference does.
-// Options (not in the reference): --storage f32|f16|bf16|f64,
+// Options (not in the reference): --storage f32|f16|f16sr|bf16|f64,
 // --streaming shift|aa, --device N, --quiet.
 #include <cstdio>
 #include <cstdlib>
@@ -12,7 +12,7 @@
 #include "lbmc.h"
 
 static void usage() {
-  fprintf(stderr, "usage: lbmc_run <input file> [--storage f32|f16|bf16|f64] [--streaming shift|aa] "
+  fprintf(stderr, "usage: lbmc_run <input file> [--storage f32|f16|f16sr|bf16|f64] [--streaming shift|aa] "
                   "[--device N] [--quiet]\n");
 }
 
@@ -31,7 +31,11 @@ int main(int argc, char **argv) {
     if (!strcmp(a, "--quiet")) {
       quiet = 1;
     } else if (!strcmp(a, "--storage")) {
-      ov.storage = !strcmp(v, "f16") ? LBMC_F16 : !strcmp(v, "bf16") ? LBMC_BF16 : !strcmp(v, "f64") ? LBMC_F64 : LBMC_F32;
+      ov.storage = !strcmp(v, "f16")     ? LBMC_F16
+                   : !strcmp(v, "f16sr") ? LBMC_F16_SR
+                   : !strcmp(v, "bf16")  ? LBMC_BF16
+                   : !strcmp(v, "f64")   ? LBMC_F64
+                                         : LBMC_F32;
       k++;
     } else if (!strcmp(a, "--streaming")) {
       ov.streaming = !strcmp(v, "shift") ? LBMC_STREAM_SHIFT : LBMC_STREAM_AA;

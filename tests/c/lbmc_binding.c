@@ -38,7 +38,7 @@ void setup_lbmc(const DomainConstant *dc, const Domain *host)
     cfg.macro_bc = dc->macro_bc;
     cfg.micro_bc = dc->micro_bc;
     cfg.init_type = LBMC_INIT_STATIC;           /* Init 0: f = w_i */
-    cfg.storage = LBMC_F32;                     /* or LBMC_F16 / LBMC_BF16 / LBMC_F64 */
+    cfg.storage = LBMC_F32;                     /* or LBMC_F16(_SR) / LBMC_BF16 / LBMC_F64 */
     cfg.compat = 0;                             /* LBMC_COMPAT_REFERENCE_AS_IS for bit-level as-is */
 
     lbmc_domain dom = {0};
