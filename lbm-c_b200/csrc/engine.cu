@@ -887,7 +887,7 @@ extern "C" lbmc_status lbmc_set_closure(lbmc_handle *h, const lbmc_mlp *m, int i
   }
   CK(cudaMemcpyAsync(h->ds.closure, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream), "upload closure");
   CK(cudaStreamSynchronize(h->stream), "upload closure");
-  h->ds.col = COL_BGK_MLP;
+  h->ds.col = iterations == 1 ? COL_BGK_MLP1 : COL_BGK_MLP;
   return LBMC_OK;
 }
 

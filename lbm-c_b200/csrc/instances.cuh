@@ -89,7 +89,7 @@ struct Launchers {
   static cudaError_t launch(const StepArgs<C> &a, const DeviceState &d, cudaStream_t st) {
     // The learned closure evaluates its network warp-wide, which the direct
     // kernel's converged warps allow: it never runs in the pipelined kernel.
-    if constexpr (COL != COL_BGK_MLP) {
+    if constexpr (!learned_closure(COL)) {
       if (d.use_pipeline) {
         auto kern = step_pipelined_kernel<L, S, COL, FORCE, BLEND, DIAG>;
         const size_t smem = (size_t)d.stages * stage_bytes(d);
@@ -146,6 +146,7 @@ struct Launchers {
       case COL_BGK_SMAG: e = launch_col<COL_BGK_SMAG>(a, d, diag, st); break;
       case COL_MRT_NC: e = launch_col<COL_MRT_NC>(a, d, diag, st); break;
       case COL_BGK_MLP: e = launch_col<COL_BGK_MLP>(a, d, diag, st); break;
+      case COL_BGK_MLP1: e = launch_col<COL_BGK_MLP1>(a, d, diag, st); break;
       default: e = launch_col<COL_MRT>(a, d, diag, st); break;
     }
     if (e != cudaSuccess) return e;

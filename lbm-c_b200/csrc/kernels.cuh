@@ -251,6 +251,8 @@ constexpr int COL_BGK_SMAG = 1;
 constexpr int COL_MRT = 2;
 constexpr int COL_MRT_NC = 3;  // MRT whose rates on rho and j are zero
 constexpr int COL_BGK_MLP = 4; // BGK family with the learned closure (Smagorinsky fallback)
+constexpr int COL_BGK_MLP1 = 5; // the same with exactly one fixed-point pass (no pass loop to carry)
+__host__ __device__ constexpr bool learned_closure(int col) { return col == COL_BGK_MLP || col == COL_BGK_MLP1; }
 
 // rho and the momentum components (the conserved moments).
 template <class L>
@@ -307,7 +309,7 @@ struct StepArgs {
   long long rows;               // Ly * Lz (pipelined kernel)
   int stages;                   // shared-memory stages (pipelined kernel)
   const uint16_t *table;        // 256 class-table entries (device memory)
-  const MlpStep *closure;       // learned closure (COL_BGK_MLP): weights
+  const MlpStep *closure;       // learned closure (COL_BGK_MLP, COL_BGK_MLP1): weights
   MlpConsts mlp;                // and its scalars
   unsigned sr_seed;             // stochastic-rounding seed of this step (sr_step_seed(t))
 };
@@ -1019,7 +1021,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
     const C usq = C(1.5) * (nd.u[0] * nd.u[0] + nd.u[1] * nd.u[1] + nd.u[2] * nd.u[2]);
     const C A0 = C(weight<L>(0)) * (nd.drho - nd.rho * usq);
     C tau = tau0;
-    if constexpr (COL == COL_BGK_SMAG || COL == COL_BGK_MLP) {
+    if constexpr (COL == COL_BGK_SMAG || learned_closure(COL)) {
       // Smagorinsky (collision.cu:445-463, q_bar zeroed): q_ab = sum e_a e_b
       // (f - f_eq) is even in e, so each pair contributes e_a e_b (S - 2A).
       C q[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, yz, xz
@@ -1055,7 +1057,11 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
         const MlpStep *cl = a.closure;
         bool in_range = participate;
         C tau_l = tau_smag;
-        for (int it = 0; it < a.mlp.iterations; it++) {
+        // One pass for COL_BGK_MLP1 is a compile-time constant: the pass
+        // loop and what it carries disappear (128 registers, no spills,
+        // against ~163 with the runtime loop).
+        const int passes = COL == COL_BGK_MLP1 ? 1 : a.mlp.iterations;
+        for (int it = 0; it < passes; it++) {
           const float ks = __fdividef(-1.5f, (float)(nd.rho * tau_l));
           float Sm[6], f[MLP_IN];
 #pragma unroll
@@ -1075,7 +1081,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       }
     }
     // 1/tau: the host's value for a uniform tau, else the local one
-    const C om = (COL == COL_BGK_SMAG || COL == COL_BGK_MLP) ? recip(tau) : a.omega;
+    const C om = (COL == COL_BGK_SMAG || learned_closure(COL)) ? recip(tau) : a.omega;
     // population 0 (e = 0)
     out[0] = nd.g[0] - omb * (om * (nd.g[0] - A0)) + omb * ft0e;
     unroll<L::NP>([&](auto pc) {
@@ -1175,7 +1181,7 @@ template <class S, int COL>
 constexpr int direct_min_blocks() {
   // FP64 arithmetic needs register pairs, the learned closure its hidden
   // layer: no cap beyond the 128 per thread that 8 resident blocks imply.
-  if (std::is_same<S, double>::value || COL == COL_BGK_MLP) return 8;
+  if (std::is_same<S, double>::value || learned_closure(COL)) return 8;
   return COL == COL_BGK_SMAG ? DIRECT_MIN_BLOCKS_SMAG : DIRECT_MIN_BLOCKS;
 }
 
@@ -1198,17 +1204,19 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
   };
   // The AA-even map needs only n; the others their sites (one block row per
   // (y, z), so the row parts are uniform across the block).
-  auto init_sites = [&](Sites &st, TiledSites &ts) {
+  // `zero` is 0; a value the compiler cannot see through makes it recompute
+  // the sites instead of keeping them live (the learned closure's stores).
+  auto init_sites = [&](Sites &st, TiledSites &ts, int zero = 0) {
     if constexpr (STREAM == STREAM_AAT_EVEN)
-      ts.init_even(blockIdx.x, threadIdx.x, blockIdx.y, blockIdx.z, a.L, Q);
+      ts.init_even(blockIdx.x + zero, threadIdx.x, blockIdx.y, blockIdx.z, a.L, Q);
     else if constexpr (STREAM == STREAM_AAT_ODD)
-      ts.init_odd(blockIdx.x, threadIdx.x, blockIdx.y, blockIdx.z, a.s, a.L, Q);
+      ts.init_odd(blockIdx.x + zero, threadIdx.x, blockIdx.y, blockIdx.z, a.s, a.L, Q);
     else if constexpr (STREAM != STREAM_AA_EVEN)
-      st.init(x, blockIdx.y, blockIdx.z, a.s, a.L);
+      st.init(x + zero, blockIdx.y, blockIdx.z, a.s, a.L);
   };
   double dv[DIAG_VALUES] = {0, 0, 0, 0, 0};
   bool nonfinite = false;
-  if constexpr (COL != COL_BGK_MLP) {
+  if constexpr (!learned_closure(COL)) {
     if (!DIAG && !active) return;
     if (active) {
       const C inv_scale = a.inv_scale, scale = a.scale;
@@ -1288,11 +1296,18 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
       collide_fluid<L, C, COL, FORCE, BLEND>(nd, a, n, fluid && cls ? a.table[cls] : 0u, out, fluid);
       if (!fluid) collide_solid(nd, out);
       if (active) {
+        // The store sites equal the load sites; recomputing them is cheaper
+        // than keeping them live across the network, which spills.
+        Sites sw;
+        TiledSites tw;
+        int zero = 0;
+        asm volatile("" : "+r"(zero));
+        init_sites(sw, tw, zero);
         if constexpr (stochastic_storage<S>())
           store_node_sr<Q, true>(out, scale, (unsigned)n ^ a.sr_seed,
-                                 [&](auto ic) { return write_at(f, st, ts, n, ic); });
+                                 [&](auto ic) { return write_at(f, sw, tw, n, ic); });
         else
-          unroll<Q>([&](auto ic) { store_dev(write_at(f, st, ts, n, ic), out[decltype(ic)::value], scale); });
+          unroll<Q>([&](auto ic) { store_dev(write_at(f, sw, tw, n, ic), out[decltype(ic)::value], scale); });
         store_and_reduce(nd, a, n, dv, nonfinite, DIAG);
       }
     }

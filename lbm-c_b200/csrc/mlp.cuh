@@ -160,6 +160,18 @@ __device__ __forceinline__ void mma_bf16_k16(float (&d)[4], const unsigned (&a)[
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// A weight fragment, loaded where it is used: the asm is volatile so that
+// the compiler neither hoists the load out of the fixed-point loop nor keeps
+// the fragment live between the two tiles (all fragments together are 32
+// registers; they come back from L1).
+__device__ __forceinline__ uint4 ldg_frag(const uint4 *p) {
+  uint4 v;
+  asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
 // silu_b of two halved pre-activations (h = z / 2): h + h tanh(h) in BF16x2.
 __device__ __forceinline__ unsigned silu_half_bf16x2(float h0, float h1) {
   const unsigned h = bf16x2_bits(__floats2bfloat162_rn(h0, h1));
@@ -171,9 +183,11 @@ __device__ __forceinline__ unsigned silu_half_bf16x2(float h0, float h1) {
 
 // Network output without the output bias b3 (and before target_scale) for
 // the calling lane's normalised inputs.  Warp-wide: all 32 lanes call it
-// together; `stage` is this warp's 128 words of shared memory.  Both
-// 16-node tiles go through each weight fragment before the next one is
-// loaded.
+// together; `stage` is this warp's 128 words of shared memory.  The two
+// 16-node tiles go through the whole network one after the other, so only
+// one tile's activations are live at a time (the step kernel keeps its
+// node state in registers meanwhile); the weight fragments of the second
+// tile are re-read from L1.
 __device__ __forceinline__ float mlp_forward_warp(const MlpStep *__restrict__ cl,
                                                   const float (&x)[MLP_IN], unsigned *stage) {
   const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
@@ -186,53 +200,46 @@ __device__ __forceinline__ float mlp_forward_warp(const MlpStep *__restrict__ cl
   r4.w = 0u;
   reinterpret_cast<uint4 *>(stage)[lane] = r4;
   __syncwarp();
-  unsigned xa[2][2];  // tile t: rows g, g + 8, column pair c
-#pragma unroll
-  for (int t = 0; t < 2; t++) {
-    xa[t][0] = stage[(16 * t + g) * 4 + c];
-    xa[t][1] = stage[(16 * t + 8 + g) * 4 + c];
-  }
-  // Layer 1 -> silu_b -> layer 2's A fragments [tile][K-tile][reg].
-  const uint4 w1 = __ldg(&cl->w1[lane]), b1 = __ldg(&cl->b1[lane]);
-  unsigned a1[2][2][4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const unsigned wj = u4_get(w1, j), bj = u4_get(b1, j);
-    const int kt = j >> 1, r = (j & 1) * 2;  // N-tile j feeds K-tile j/2, regs r, r + 1
-#pragma unroll
-    for (int t = 0; t < 2; t++) {
-      float d[4];
-      mma_bf16_k8(d, xa[t][0], xa[t][1], wj, bf16_lo(bj), bf16_hi(bj));
-      a1[t][kt][r] = silu_half_bf16x2(d[0], d[1]);
-      a1[t][kt][r + 1] = silu_half_bf16x2(d[2], d[3]);
-    }
-  }
-  // Layer 2 -> silu_b -> layer 3's A fragments.
-  const uint4 b2 = __ldg(&cl->b2[lane]);
-  unsigned a2[2][2][4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    const uint4 w2 = __ldg(&cl->w2[j][lane]);
-    const unsigned bj = u4_get(b2, j);
-    const int kt = j >> 1, r = (j & 1) * 2;
-#pragma unroll
-    for (int t = 0; t < 2; t++) {
-      float d[4];
-      mma_bf16_k16_c(d, a1[t][0], w2.x, w2.y, bf16_lo(bj), bf16_hi(bj));
-      mma_bf16_k16(d, a1[t][1], w2.z, w2.w);
-      a2[t][kt][r] = silu_half_bf16x2(d[0], d[1]);
-      a2[t][kt][r + 1] = silu_half_bf16x2(d[2], d[3]);
-    }
-  }
-  // Layer 3: column 0 of the accumulator is the output; lanes with c == 0
-  // hold rows g (d[0]) and g + 8 (d[2]).
-  const uint4 w3 = __ldg(&cl->w3[lane]);
   float out[4];  // entry 2t + h: tile t, row g + 8h
 #pragma unroll
   for (int t = 0; t < 2; t++) {
+    const unsigned xa0 = stage[(16 * t + g) * 4 + c], xa1 = stage[(16 * t + 8 + g) * 4 + c];
+    // Layer 1 -> silu_b -> layer 2's A fragments [K-tile][reg].
+    unsigned a1[2][4];
+    {
+      const uint4 w1 = ldg_frag(&cl->w1[lane]), b1 = ldg_frag(&cl->b1[lane]);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const unsigned wj = u4_get(w1, j), bj = u4_get(b1, j);
+        const int kt = j >> 1, r = (j & 1) * 2;  // N-tile j feeds K-tile j/2, regs r, r + 1
+        float d[4];
+        mma_bf16_k8(d, xa0, xa1, wj, bf16_lo(bj), bf16_hi(bj));
+        a1[kt][r] = silu_half_bf16x2(d[0], d[1]);
+        a1[kt][r + 1] = silu_half_bf16x2(d[2], d[3]);
+      }
+    }
+    // Layer 2 -> silu_b -> layer 3's A fragments.
+    unsigned a2[2][4];
+    {
+      const uint4 b2 = ldg_frag(&cl->b2[lane]);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint4 w2 = ldg_frag(&cl->w2[j][lane]);
+        const unsigned bj = u4_get(b2, j);
+        const int kt = j >> 1, r = (j & 1) * 2;
+        float d[4];
+        mma_bf16_k16_c(d, a1[0], w2.x, w2.y, bf16_lo(bj), bf16_hi(bj));
+        mma_bf16_k16(d, a1[1], w2.z, w2.w);
+        a2[kt][r] = silu_half_bf16x2(d[0], d[1]);
+        a2[kt][r + 1] = silu_half_bf16x2(d[2], d[3]);
+      }
+    }
+    // Layer 3: column 0 of the accumulator is the output; lanes with c == 0
+    // hold rows g (d[0]) and g + 8 (d[2]).
+    const uint4 w3 = ldg_frag(&cl->w3[lane]);
     float d[4];
-    mma_bf16_k16_c(d, a2[t][0], w3.x, w3.y, 0.f, 0.f);
-    mma_bf16_k16(d, a2[t][1], w3.z, w3.w);
+    mma_bf16_k16_c(d, a2[0], w3.x, w3.y, 0.f, 0.f);
+    mma_bf16_k16(d, a2[1], w3.z, w3.w);
     out[2 * t] = d[0];
     out[2 * t + 1] = d[2];
   }
