@@ -509,6 +509,22 @@ __device__ __forceinline__ C recip(C x) {
   }
 }
 
+// Rounded multiply and fused multiply-add with the fusion spelled out: the
+// compiler fuses a multiply and an add of an expression or not depending on
+// the code around it, so an expression that several kernels inline
+// (different streaming layouts, the two step kernels) is written with these
+// where both forms are possible, and every kernel computes the same bits.
+template <class C>
+__device__ __forceinline__ C mul_rn(C x, C y) {
+  if constexpr (std::is_same<C, float>::value) return __fmul_rn(x, y);
+  else return __dmul_rn(x, y);
+}
+template <class C>
+__device__ __forceinline__ C fma_rn(C x, C y, C z) {
+  if constexpr (std::is_same<C, float>::value) return __fmaf_rn(x, y, z);
+  else return __fma_rn(x, y, z);
+}
+
 // rho = 1 + sum g, u = sum e g / rho (LBM-C/solver.cu:96-108).
 template <class L, class C>
 __device__ __forceinline__ void moments(Node<L, C> &nd) {
@@ -890,7 +906,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       constexpr int i = decltype(ic)::value;
       const C eu = edot<L, i>(nd.u);
       if (!a.force[0]) {  // uniform force: the host's per-population terms
-        even = a.guo_a[i] * eu - a.guo_b[i] * uF;
+        even = fma_rn(a.guo_a[i], eu, -mul_rn(a.guo_b[i], uF));
         odd = a.guo_odd[i];
       } else {
         const C wp = C(weight<L>(i)) * pre;
@@ -1042,7 +1058,7 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
       C qhat = r2 * (fabs(q[0]) + fabs(q[1]) + C(2) * fabs(q[3]));
       if (L::DIM > 2) qhat += r2 * (fabs(q[2]) + C(2) * (fabs(q[4]) + fabs(q[5])));
       const C k = C(2) * r2 * a.c_smag * a.c_smag * (C(9) * recip(nd.rho));
-      const C tau_smag = tau0 + C(0.5) * (sqrt(tau0 * tau0 + k * qhat) - tau0);
+      const C tau_smag = tau0 + C(0.5) * (sqrt(fma_rn(k, qhat, mul_rn(tau0, tau0))) - tau0);
       if constexpr (COL == COL_BGK_SMAG) {
         tau = tau_smag;
       } else {
