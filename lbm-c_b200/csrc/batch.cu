@@ -113,7 +113,7 @@ __device__ __forceinline__ void batch_node(S *pop, long long pitch, int k, int x
   } else {
     moments(nd);
     // a.B is this domain's porosity array; only partial nodes read it.
-    collide_fluid<L, float, COL_BGK, true, BLEND>(nd, a, k, cls == 2 ? ENTRY_PARTIAL : 0u, out);
+    collide_fluid<L, float, COL_BGK, true, BLEND, true>(nd, a, k, cls == 2 ? ENTRY_PARTIAL : 0u, out);
   }
   // The store slots equal the load slots; recomputing them from the six
   // coordinates is cheaper than keeping nine addresses live across the

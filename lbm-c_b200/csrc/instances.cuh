@@ -35,7 +35,6 @@ struct Launchers {
     a.n = (int)d.n;
     a.tau = (C)d.tau;
     a.omega = (C)(1.0 / d.tau);
-    set_uniform_guo<L, C>(a.guo_a, a.guo_b, a.guo_odd, d.tau, d.force_u);
     // MRT rates pre-divided by the moment norms D_k = sum_i M_ki^2.
     for (int k = 0; k < 15; k++) a.s_mrt[k] = k < L::Q ? (C)(d.s_mrt[k] / (double)L::mnorm(k)) : C(0);
     a.c_smag = (C)d.c_smag;

@@ -295,9 +295,10 @@ struct StepArgs {
   int n;
   C tau;
   C omega;    // 1/tau
-  // Guo source terms of a uniform force F (force[] all null), per population
+  // Guo source terms of the batched domains' uniform force F, per population
   // i, with pre = 1 - 1/(2 tau): guo_a = 9 w_i pre (e_i.F), guo_b = 3 w_i pre,
-  // guo_odd = 3 w_i pre (e_i.F); the even part is guo_a (e_i.u) - guo_b (u.F).
+  // guo_odd = 3 w_i pre (e_i.F); the even part is guo_a (e_i.u) - guo_b (u.F)
+  // (collide_fluid with GUO_UNIFORM).
   C guo_a[15], guo_b[15], guo_odd[15];
   C s_mrt[15];
   C c_smag;
@@ -866,7 +867,11 @@ __device__ __forceinline__ void mrt_d3q15(const Node<D3Q15, C> &nd, const C *sra
 // pair.  Post-collision deviations go to out[].
 // `participate` (learned closure only): false for the lanes that only
 // accompany the warp-wide network evaluation (solid or out-of-range nodes).
-template <class L, class C, int COL, bool FORCE, bool BLEND>
+// GUO_UNIFORM (the batched domains, whose force is always uniform): the
+// Guo source from the host's per-population terms guo_a / guo_b / guo_odd.
+// The single-domain kernels keep the per-node form, whose arithmetic is the
+// same in every instantiation (shift and AA layouts, both step kernels).
+template <class L, class C, int COL, bool FORCE, bool BLEND, bool GUO_UNIFORM = false>
 __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> &a, int n,
                                               unsigned entry, C (&out)[L::Q], bool participate = true) {
   constexpr int Q = L::Q;
@@ -895,25 +900,23 @@ __device__ __forceinline__ void collide_fluid(Node<L, C> &nd, const StepArgs<C> 
     nd.u[0] += h * F[0];
     nd.u[1] += h * F[1];
     if (L::DIM > 2) nd.u[2] += h * F[2];
-    if (a.force[0]) pre = C(1) - recip(C(2) * tau0);
+    if constexpr (!GUO_UNIFORM) pre = C(1) - recip(C(2) * tau0);
     uF = nd.u[0] * F[0] + nd.u[1] * F[1] + (L::DIM > 2 ? nd.u[2] * F[2] : C(0));
   }
   const C omb = C(1) - B;
   // Guo source (collision.cu:82-99): F_i = w_i pre (3 (e_i.F - u.F) + 9 (e_i.u)(e_i.F)),
   // even part w pre (9 (e.u)(e.F) - 3 u.F), odd part 3 w pre e.F.
   auto guo_parts = [&](auto ic, C &even, C &odd) {
-    if constexpr (FORCE) {
+    if constexpr (FORCE && GUO_UNIFORM) {
       constexpr int i = decltype(ic)::value;
-      const C eu = edot<L, i>(nd.u);
-      if (!a.force[0]) {  // uniform force: the host's per-population terms
-        even = fma_rn(a.guo_a[i], eu, -mul_rn(a.guo_b[i], uF));
-        odd = a.guo_odd[i];
-      } else {
-        const C wp = C(weight<L>(i)) * pre;
-        const C eF = edot<L, i>(F);
-        even = wp * (C(9) * eu * eF - C(3) * uF);
-        odd = wp * C(3) * eF;
-      }
+      even = fma_rn(a.guo_a[i], edot<L, i>(nd.u), -mul_rn(a.guo_b[i], uF));
+      odd = a.guo_odd[i];
+    } else if constexpr (FORCE) {
+      constexpr int i = decltype(ic)::value;
+      const C wp = C(weight<L>(i)) * pre;
+      const C eF = edot<L, i>(F), eu = edot<L, i>(nd.u);
+      even = wp * (C(9) * eu * eF - C(3) * uF);
+      odd = wp * C(3) * eF;
     } else {
       even = 0;
       odd = 0;
