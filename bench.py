@@ -674,6 +674,22 @@ def run_ours(args, world, rank, local):
                       " freeing); slowest of the timed jobs",
                "seconds_per_job": [round(x, 4) for x in times], "phases": phases}
 
+    # Reduced-precision storage: the velocity error of this storage against
+    # an FP64-storage run of the same workload and step count (outside the
+    # timed region).
+    accuracy = None
+    if rank == 0 and STORAGE_BYTES[args.storage] == 2 and args.accuracy_steps > 0 and mlp is None:
+        fields = {}
+        for st in ("f64", args.storage):
+            e = workloads.engine_for(lbmc, w, st, device=local, kernel=kernel, streaming=streaming)
+            e.iterate(args.accuracy_steps, lbmc.STORE_MACROS | lbmc.SYNC)
+            fields[st] = e.u()
+            e.close()
+        u64, u2 = fields["f64"], fields[args.storage]
+        accuracy = {"steps": args.accuracy_steps, "reference": "f64 storage, same engine and workload",
+                    "u_rel_l2": float(np.linalg.norm(u2 - u64) / np.linalg.norm(u64)),
+                    "u_rel_max": float(np.abs(u2 - u64).max() / np.abs(u64).max())}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -708,6 +724,7 @@ def run_ours(args, world, rank, local):
             "e2e": e2e,
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
+            "accuracy_vs_f64": accuracy,
             "diag": {"mass": diag.mass, "kinetic_energy": diag.kinetic_energy,
                      "nonfinite": diag.nonfinite},
         }
@@ -742,6 +759,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--ref-nz", type=int, default=32)
+    ap.add_argument("--accuracy-steps", type=int, default=5000,
+                    help="2-byte storages: steps of the FP64 comparison run reported in the line "
+                         "(0 = none)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
