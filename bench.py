@@ -26,6 +26,7 @@ one domain), so scaling is weak and there is no collective in the data path.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -632,11 +633,22 @@ def run_ours(args, world, rank, local):
         times, phases = [], []
         h2d = w.host_bytes()
         d2h = w.n * 8 * (1 + w.dim)
-        # Host output arrays exist before the job, like the input arrays
-        # (LBM-C fills the host Domain arrays that set-up allocated,
-        # index.cu:196-216); touched once so that no job pays page faults.
-        rho_out = np.zeros(w.n)
-        u_out = np.zeros((w.dim, w.n))
+
+        # Inputs and outputs in pinned host memory: the workload's arrays
+        # are copied into page-locked buffers once, before any job, and the
+        # outputs exist before the job too (LBM-C fills the host Domain
+        # arrays that set-up allocated, index.cu:196-216).
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, pin_memory=True)
+            out = t.numpy()
+            out[...] = a
+            keep_pinned.append(t)
+            return out
+        keep_pinned = []
+        w = dataclasses.replace(w, arrays={k: (None if v is None else pinned(np.ascontiguousarray(v)))
+                                           for k, v in w.arrays.items()})
+        rho_out = pinned(np.zeros(w.n))
+        u_out = pinned(np.zeros((w.dim, w.n)))
         for k in range(args.e2e_reps + 1):
             torch.cuda.synchronize(device)
             t = time.perf_counter()
@@ -664,7 +676,7 @@ def run_ours(args, world, rank, local):
         e2e_rate, _ = aggregate_rate(w.n * E2E_STEPS, max(times), world, device)
         # Each job moves its inputs in once and its result out once; per step
         # that is the job's bytes over its steps.
-        e2e = {"value": e2e_rate / 1e9, "unit": UNIT,
+        e2e = {"value": e2e_rate / 1e9, "unit": UNIT, "host_memory": "pinned (page-locked) input and output arrays",
                "h2d_bytes_per_step": int(round(h2d / E2E_STEPS)),
                "d2h_bytes_per_step": int(round(d2h / E2E_STEPS)),
                "h2d_bytes_per_job": int(h2d), "d2h_bytes_per_job": int(d2h),
