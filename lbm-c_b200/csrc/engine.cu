@@ -510,9 +510,22 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   const long long n = d.n;
   const int q = d.q, cs = h->ops->csize, ss = h->ops->ssize;
 
+  // The node classes are packed on the host's cores while this thread
+  // uploads rho and u (DMA): the two take similar times and do not depend
+  // on each other.  The packing thread reads only cfg and dom.
   HostClasses hc;
-  TRY(build_classes(cfg, dom, n, hc));
-  memcpy(d.table, hc.table, sizeof(d.table));
+  lbmc_status cls_status = LBMC_OK;
+  std::string cls_error;
+  std::thread cls_thread([&] {
+    cls_status = build_classes(cfg, dom, n, hc);
+    if (cls_status != LBMC_OK) cls_error = lbmc_last_error();
+  });
+  struct Joiner {
+    std::thread &t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } joiner{cls_thread};
 
   d.tau = cfg->tau;
   d.c_smag = cfg->c_smag;
@@ -527,7 +540,6 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     if (conserved_zero) d.col = COL_MRT_NC;
   }
   d.forcing = cfg->forcing ? 1 : 0;
-  d.blend = hc.any_partial ? 1 : 0;
 
   TRYCUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
   h->stream = h->own_stream;
@@ -537,7 +549,6 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   d.pitch = (n + align - 1) / align * align;
   TRY(dev_alloc(h, &d.f, (size_t)d.pitch * q * ss, "populations"));
   TRY(dev_alloc(h, &d.cls, (size_t)n, "node classes"));
-  TRYCUDA(cudaMemcpy(d.cls, hc.cls.data(), n, cudaMemcpyHostToDevice), "upload classes");
 
   // rho - 1 and u: prescribed input (macro BC) and stored output.
   TRY(dev_alloc(h, &d.rho, (size_t)n * cs, "rho"));
@@ -549,6 +560,16 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     }
   }
   if (d.dim == 2) d.u[2] = d.u[1];  // never written for D2Q9; keeps pointers valid
+
+  cls_thread.join();
+  if (cls_status != LBMC_OK) {
+    release(h);
+    set_last_error(cls_error);
+    return cls_status;
+  }
+  memcpy(d.table, hc.table, sizeof(d.table));
+  d.blend = hc.any_partial ? 1 : 0;
+  TRYCUDA(cudaMemcpy(d.cls, hc.cls.data(), n, cudaMemcpyHostToDevice), "upload classes");
 
   if (hc.any_partial) {
     TRY(dev_alloc(h, &d.B, (size_t)n * cs, "porosity"));
