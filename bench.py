@@ -402,7 +402,7 @@ class ReferenceTimer:
         if w.dim == 2:
             ly_c, lz_c = ly, 1
         else:
-            ly_c, lz_c = ly, max(1, min(nz, lz))
+            ly_c, lz_c = ly, (lz if nz <= 0 else max(1, min(nz, lz)))
         n = lx * ly_c * lz_c
         a = w.arrays
 
@@ -425,7 +425,9 @@ class ReferenceTimer:
         self.ref = Reference(case, variant, nthreads=threads)
         self.n, self.threads = n, threads
         shape = f"{lx}x{ly_c}" if w.dim == 2 else f"{lx}x{ly_c}x{lz_c}"
-        self.sample = f"{shape} crop of the workload, FP64, {variant} reference step"
+        whole = (lx, ly_c, lz_c)[:w.dim] == tuple(w.length[:w.dim])
+        self.sample = (f"the whole {shape} workload" if whole else f"{shape} crop of the workload") + \
+            f", FP64, {variant} reference step"
 
     def rate(self, steps: int) -> float:
         """Lattice updates per second over `steps` reference steps."""
@@ -529,9 +531,10 @@ def run_reference_arm(args, world, rank):
     t = time.perf_counter()
     timer.ref.run(1)
     total = (args.steps + max(1, args.warmup)) * (time.perf_counter() - t)
-    if w.dim == 3 and total > REF_ARM_SECONDS and args.ref_nz > 1:
+    lz_now = timer.n // (w.length[0] * w.length[1]) if w.dim == 3 else 1
+    if w.dim == 3 and total > REF_ARM_SECONDS and lz_now > 1:
         timer.close()
-        timer = ReferenceTimer(w, max(1, int(args.ref_nz * REF_ARM_SECONDS / total)), threads)
+        timer = ReferenceTimer(w, max(1, int(lz_now * REF_ARM_SECONDS / total)), threads)
     timer.rate(max(1, args.warmup))
     t_total, steps = 0.0, 0
     for _ in range(args.steps):
@@ -772,7 +775,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--ref-nz", type=int, default=32)
+    ap.add_argument("--ref-nz", type=int, default=0,
+                    help="reference step on the first NZ planes of a 3-D workload (0 = all; the "
+                         "reference arm still crops if its run would pass %d s)" % REF_ARM_SECONDS)
     ap.add_argument("--accuracy-steps", type=int, default=5000,
                     help="2-byte storages: steps of the FP64 comparison run reported in the line "
                          "(0 = none)")
