@@ -7,6 +7,10 @@
 
 namespace lbmc {
 
+// Shared memory of the pipelined kernel's stages, per block: with
+// PIPE_MIN_BLOCKS resident blocks, 4 x 48 KB of the SM's 228 KB.
+constexpr long long PIPE_STAGE_BUDGET = 48 * 1024;
+
 template <class L, class S>
 struct Launchers {
   using C = typename Storage<S>::C;
@@ -73,7 +77,7 @@ struct Launchers {
     return d.pipeline && (d.L[0] * sizeof(S)) % 16 == 0 && 2 * stage_bytes(d) <= 200 * 1024;
   }
   static int pipe_stages(const DeviceState &d) {
-    long long st = (96 * 1024) / (long long)stage_bytes(d);
+    long long st = PIPE_STAGE_BUDGET / (long long)stage_bytes(d);
     if (st < 2) st = 2;
     if (st > PIPE_MAX_STAGES) st = PIPE_MAX_STAGES;
     return (int)st;
