@@ -11,15 +11,19 @@
 // compute_residual (LBM-C/index.cu:196-216, 387-439).
 #include <cuda_runtime.h>
 
+#include <sys/mman.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
 #include <climits>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -117,9 +121,37 @@ int parallel_for(long long n, F body) {
   return t;
 }
 
+// Host scratch of the class packing: left uninitialised, so that the
+// parallel passes touch its pages first (the page faults spread over the
+// cores), and 2 MB aligned with a huge-page hint, so that where the kernel
+// has transparent huge pages a 16 M-node domain faults a few dozen pages
+// instead of ~12,000.
+template <class T>
+class HostBuffer {
+ public:
+  HostBuffer() = default;
+  HostBuffer(const HostBuffer &) = delete;
+  HostBuffer &operator=(const HostBuffer &) = delete;
+  ~HostBuffer() { std::free(p_); }
+  bool allocate(size_t count) {
+    constexpr size_t HUGE_PAGE = 2u << 20;
+    const size_t bytes = (count * sizeof(T) + HUGE_PAGE - 1) / HUGE_PAGE * HUGE_PAGE;
+    std::free(p_);
+    p_ = static_cast<T *>(std::aligned_alloc(HUGE_PAGE, bytes ? bytes : HUGE_PAGE));
+    if (p_ && bytes) madvise(p_, bytes, MADV_HUGEPAGE);
+    return p_ != nullptr;
+  }
+  T *data() { return p_; }
+  const T *data() const { return p_; }
+  T &operator[](size_t k) { return p_[k]; }
+
+ private:
+  T *p_ = nullptr;
+};
+
 // Host-side packing of the per-node inputs.
 struct HostClasses {
-  std::vector<uint8_t> cls;
+  HostBuffer<uint8_t> cls;
   uint16_t table[256];
   int nclasses = 2;
   std::vector<int> sf_nodes;
@@ -171,8 +203,9 @@ static double default_scale(int storage) {
   return storage == LBMC_F16 || storage == LBMC_F16_SR ? 1024.0 : 1.0;
 }
 
-// Checks a configuration and domain without touching the GPU.
-extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *dom) {
+// The configuration checks of lbmc_validate (everything but the per-node
+// arrays).
+static lbmc_status validate_config(const lbmc_config *cfg, const lbmc_domain *dom) {
   if (!cfg) return fail(LBMC_ERR_INVALID_ARG, "config is NULL");
   if (cfg->lattice != LBMC_D2Q9 && cfg->lattice != LBMC_D3Q15)
     return fail(LBMC_ERR_INVALID_ARG, "unknown lattice %d", cfg->lattice);
@@ -221,43 +254,72 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     return fail(LBMC_ERR_INVALID_ARG, "macro_bc is on but domain.macro_bc is NULL");
   if (cfg->micro_bc && !dom->micro_bc)
     return fail(LBMC_ERR_INVALID_ARG, "micro_bc is on but domain.micro_bc is NULL");
-  // Per-node checks; the first failing node in node order is reported.
-  // Returns 0 if node k is fine, else writes the message.
-  const bool have_u = dom->u[0] && dom->u[1] && (dim == 2 || dom->u[2]);
-  auto check_node = [&](long long k, bool &needs_rho, char *msg, size_t len) -> bool {
-    const double B = dom->geometry ? dom->geometry[k] : 0.0;
-    if (!std::isfinite(B)) {
-      snprintf(msg, len, "Porosity at node %lld is not finite", k);
+  return LBMC_OK;
+}
+
+// The per-node checks of lbmc_validate for node k: false (and the message)
+// at a bad node; needs_rho is set where a MacroBC code prescribes rho.
+static bool node_ok(const lbmc_config *cfg, const lbmc_domain *dom, long long k, bool have_u, bool &needs_rho,
+                    char *msg, size_t len) {
+  const double B = dom->geometry ? dom->geometry[k] : 0.0;
+  if (!std::isfinite(B)) {
+    snprintf(msg, len, "Porosity at node %lld is not finite", k);
+    return false;
+  }
+  if (B >= 1) return true;
+  if (cfg->macro_bc) {
+    const int c = dom->macro_bc[k];
+    if (c < 0 || c > 15) {
+      snprintf(msg, len, "MacroBC code %d at node %lld is outside 0..15", c, k);
       return false;
     }
-    if (B >= 1) return true;
-    if (cfg->macro_bc) {
-      const int c = dom->macro_bc[k];
-      if (c < 0 || c > 15) {
-        snprintf(msg, len, "MacroBC code %d at node %lld is outside 0..15", c, k);
-        return false;
-      }
-      if (macro_mask(c) & 0x8) needs_rho = true;
-      if ((macro_mask(c) & 0x7) && !have_u) {
-        snprintf(msg, len, "MacroBC code %d needs the velocity fields", c);
-        return false;
-      }
+    if (macro_mask(c) & 0x8) needs_rho = true;
+    if ((macro_mask(c) & 0x7) && !have_u) {
+      snprintf(msg, len, "MacroBC code %d needs the velocity fields", c);
+      return false;
     }
-    if (cfg->micro_bc) {
-      const int c = dom->micro_bc[k];
-      const int maxc = cfg->lattice == LBMC_D2Q9 ? 8 : 12;
-      if (c < 0 || c > maxc) {
-        snprintf(msg, len, "MicroBC code %d at node %lld is outside 0..%d", c, k, maxc);
-        return false;
-      }
-      // micro_bc.cuh:7-8 leaves D2Q9 codes 3 and 4 as NULL entries.
-      if (cfg->lattice == LBMC_D2Q9 && (c == 3 || c == 4)) {
-        snprintf(msg, len, "MicroBC code %d is undefined for D2Q9 (node %lld)", c, k);
-        return false;
-      }
+  }
+  if (cfg->micro_bc) {
+    const int c = dom->micro_bc[k];
+    const int maxc = cfg->lattice == LBMC_D2Q9 ? 8 : 12;
+    if (c < 0 || c > maxc) {
+      snprintf(msg, len, "MicroBC code %d at node %lld is outside 0..%d", c, k, maxc);
+      return false;
     }
-    return true;
-  };
+    // micro_bc.cuh:7-8 leaves D2Q9 codes 3 and 4 as NULL entries.
+    if (cfg->lattice == LBMC_D2Q9 && (c == 3 || c == 4)) {
+      snprintf(msg, len, "MicroBC code %d is undefined for D2Q9 (node %lld)", c, k);
+      return false;
+    }
+  }
+  return true;
+}
+
+static bool have_velocity(const lbmc_config *cfg, const lbmc_domain *dom) {
+  return dom->u[0] && dom->u[1] && (lattice_dim(cfg->lattice) == 2 || dom->u[2]);
+}
+
+// The status of the per-node checks, from the first bad node in node order
+// (LLONG_MAX: none) and whether some node prescribes rho.
+static lbmc_status node_status(const lbmc_config *cfg, const lbmc_domain *dom, long long bad, bool needs_rho) {
+  if (bad != LLONG_MAX) {
+    char msg[160];
+    bool unused = false;
+    node_ok(cfg, dom, bad, have_velocity(cfg, dom), unused, msg, sizeof(msg));
+    return fail(LBMC_ERR_INVALID_ARG, "%s", msg);
+  }
+  if (needs_rho && !dom->rho) return fail(LBMC_ERR_INVALID_ARG, "a MacroBC code prescribes rho but domain.rho is NULL");
+  return LBMC_OK;
+}
+
+// Checks a configuration and domain without touching the GPU; the first
+// failing node in node order is reported.
+extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *dom) {
+  lbmc_status st = validate_config(cfg, dom);
+  if (st != LBMC_OK) return st;
+  long long n = 1;
+  for (int d = 0; d < lattice_dim(cfg->lattice); d++) n *= cfg->length[d];
+  const bool have_u = have_velocity(cfg, dom);
   struct Chunk {
     long long bad = LLONG_MAX;
     bool needs_rho = false;
@@ -266,7 +328,7 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
   parallel_for(n, [&](long long b, long long e, int c) {
     char msg[160];
     for (long long k = b; k < e; k++)
-      if (!check_node(k, chunks[c].needs_rho, msg, sizeof(msg))) {
+      if (!node_ok(cfg, dom, k, have_u, chunks[c].needs_rho, msg, sizeof(msg))) {
         chunks[c].bad = k;
         break;
       }
@@ -277,33 +339,31 @@ extern "C" lbmc_status lbmc_validate(const lbmc_config *cfg, const lbmc_domain *
     needs_rho = needs_rho || c.needs_rho;
     bad = std::min(bad, c.bad);
   }
-  if (bad != LLONG_MAX) {
-    char msg[160];
-    bool unused = false;
-    check_node(bad, unused, msg, sizeof(msg));
-    return fail(LBMC_ERR_INVALID_ARG, "%s", msg);
-  }
-  if (needs_rho && !dom->rho) return fail(LBMC_ERR_INVALID_ARG, "a MacroBC code prescribes rho but domain.rho is NULL");
-  return LBMC_OK;
+  return node_status(cfg, dom, bad, needs_rho);
 }
 
 // Packs Porosity / MacroBC / MicroBC into class bytes (host only, no GPU).
 // Class ids >= 2 go to the distinct (MacroBC, MicroBC, partial) entries in
 // the order of their first node; the pass runs on the host's cores.
+// With `check`, the per-node checks of lbmc_validate run in the same pass
+// over the input arrays (lbmc_init reads them once).
 static lbmc_status build_classes(const lbmc_config *cfg, const lbmc_domain *dom, long long n,
-                                 HostClasses &hc) {
-  hc.cls.resize(n);
+                                 HostClasses &hc, bool check) {
+  HostBuffer<uint16_t> key;
+  if (!hc.cls.allocate(n) || !key.allocate(n)) return fail(LBMC_ERR_ALLOC, "host allocation of %lld node classes", n);
   memset(hc.table, 0, sizeof(hc.table));
   const bool blend = cfg->collision_type == LBMC_NTPOR || cfg->collision_type == LBMC_MRTPOR;
   constexpr int KEYS = 512;            // macro (4 bits) | micro << 4 (4 bits) | partial << 8
   constexpr uint16_t SOLID_KEY = 0xFFFF;
-  std::unique_ptr<uint16_t[]> key(new uint16_t[n]);
   struct Chunk {
     long long first[KEYS];
     bool any_partial = false;
     std::vector<int> sf_nodes;
     std::vector<uint8_t> sf_face;
+    long long bad = LLONG_MAX;
+    bool needs_rho = false;
   };
+  const bool have_u = have_velocity(cfg, dom);
   std::vector<std::unique_ptr<Chunk>> chunks(32);
   for (auto &c : chunks) {
     c.reset(new Chunk());
@@ -311,7 +371,12 @@ static lbmc_status build_classes(const lbmc_config *cfg, const lbmc_domain *dom,
   }
   parallel_for(n, [&](long long b, long long e, int ci) {
     Chunk &c = *chunks[ci];
+    char msg[160];
     for (long long k = b; k < e; k++) {
+      if (check && !node_ok(cfg, dom, k, have_u, c.needs_rho, msg, sizeof(msg))) {
+        c.bad = k;
+        break;
+      }
       const double B = dom->geometry ? dom->geometry[k] : 0.0;
       if (B >= 1) {  // LBM-C/solver.cu:67-72
         key[k] = SOLID_KEY;
@@ -330,6 +395,16 @@ static lbmc_status build_classes(const lbmc_config *cfg, const lbmc_domain *dom,
       if (entry && c.first[entry] == LLONG_MAX) c.first[entry] = k;
     }
   });
+  if (check) {
+    bool needs_rho = false;
+    long long bad = LLONG_MAX;
+    for (auto &c : chunks) {
+      needs_rho = needs_rho || c->needs_rho;
+      bad = std::min(bad, c->bad);
+    }
+    const lbmc_status st = node_status(cfg, dom, bad, needs_rho);
+    if (st != LBMC_OK) return st;
+  }
   // Ids by first appearance, as a sequential scan would give them.
   std::vector<std::pair<long long, int>> order;
   for (int e = 1; e < KEYS; e++) {
@@ -369,7 +444,7 @@ extern "C" lbmc_status lbmc_classify(const lbmc_config *cfg, const lbmc_domain *
   long long n = 1;
   for (int d = 0; d < lattice_dim(cfg->lattice); d++) n *= cfg->length[d];
   HostClasses hc;
-  s = build_classes(cfg, dom, n, hc);
+  s = build_classes(cfg, dom, n, hc, false);
   if (s != LBMC_OK) return s;
   if (cls_out) memcpy(cls_out, hc.cls.data(), n);
   if (table_out) memcpy(table_out, hc.table, sizeof(hc.table));
@@ -478,10 +553,26 @@ static void release(lbmc_handle *h) {
     }                                             \
   } while (0)
 
+// SM clock of a device in kHz, queried once per device and process.
+static long long device_clock_khz(int device) {
+  static std::mutex mu;
+  static std::vector<long long> khz_of;
+  std::lock_guard<std::mutex> lock(mu);
+  if (device >= (int)khz_of.size()) khz_of.resize(device + 1, 0);
+  if (khz_of[device] == 0) {
+    int khz = 0;
+    cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device);
+    khz_of[device] = khz > 0 ? khz : 2000000;
+  }
+  return khz_of[device];
+}
+
 extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom, lbmc_handle **out) {
   if (!out) return fail(LBMC_ERR_INVALID_ARG, "lbmc_init: out is NULL");
   *out = nullptr;
-  lbmc_status st = lbmc_validate(cfg, dom);
+  // The per-node checks run with the class packing below, on the host's
+  // cores while the uploads run.
+  lbmc_status st = validate_config(cfg, dom);
   if (st != LBMC_OK) return st;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -510,23 +601,6 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   const long long n = d.n;
   const int q = d.q, cs = h->ops->csize, ss = h->ops->ssize;
 
-  // The node classes are packed on the host's cores while this thread
-  // uploads rho and u (DMA): the two take similar times and do not depend
-  // on each other.  The packing thread reads only cfg and dom.
-  HostClasses hc;
-  lbmc_status cls_status = LBMC_OK;
-  std::string cls_error;
-  std::thread cls_thread([&] {
-    cls_status = build_classes(cfg, dom, n, hc);
-    if (cls_status != LBMC_OK) cls_error = lbmc_last_error();
-  });
-  struct Joiner {
-    std::thread &t;
-    ~Joiner() {
-      if (t.joinable()) t.join();
-    }
-  } joiner{cls_thread};
-
   d.tau = cfg->tau;
   d.c_smag = cfg->c_smag;
   for (int k = 0; k < 15; k++) d.s_mrt[k] = k < q ? cfg->tau_mrt[k] : 0.0;
@@ -544,22 +618,91 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   TRYCUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
   h->stream = h->own_stream;
 
-  // Populations: Q arrays, each padded to a 256-byte boundary.
-  const long long align = 256 / ss;
-  d.pitch = (n + align - 1) / align * align;
-  TRY(dev_alloc(h, &d.f, (size_t)d.pitch * q * ss, "populations"));
-  TRY(dev_alloc(h, &d.cls, (size_t)n, "node classes"));
+  // Every device-side wait gives up after about two seconds.
+  d.timeout_cycles = device_clock_khz(cfg->device) * 1000LL * 2;
+  d.aa = cfg->streaming == LBMC_STREAM_AA ? 1 : 0;
+  // The tiled AA layout needs whole 64-node tiles along x (one direct-kernel
+  // block each) and element indices over all Q arrays below 2^32 (its row
+  // and x offsets are 32-bit); other domains keep the plain AA layout.
+  d.tiled = d.aa && d.L[0] % lbmc::TILE == 0 && (long long)q * n < (1ll << 32) ? 1 : 0;
+  d.pipeline = cfg->kernel == LBMC_KERNEL_PIPELINED ? 2 : 0;
+  TRYCUDA(h->ops->plan(d), "kernel planning");
+  if (cfg->kernel == LBMC_KERNEL_PIPELINED && !d.use_pipeline) {
+    release(h);
+    return fail(LBMC_ERR_UNSUPPORTED,
+                "the bulk-copy pipeline needs Lx * element size to be a multiple of 16 bytes "
+                "and two stages of Q rows to fit in shared memory");
+  }
+  h->nblocks = d.nblocks;
+
+  // The buffers every handle holds come from one cudaMalloc, carved at
+  // 256-byte boundaries: each cudaMalloc of a large buffer measured 1-5 ms
+  // (page mapping in the driver), about as long as the upload of a field.
+  {
+    // Populations: Q arrays, each padded to a 256-byte boundary.
+    const long long align = 256 / ss;
+    d.pitch = (n + align - 1) / align * align;
+    const long long stage_n = std::min(n, FETCH_CHUNK);
+    const size_t sizes[] = {(size_t)d.pitch * q * ss,                                     // populations
+                            (size_t)n,                                                    // node classes
+                            (size_t)n * cs, (size_t)n * cs, (size_t)n * cs,               // rho - 1, u_x, u_y
+                            d.dim > 2 ? (size_t)n * cs : 0,                               // u_z
+                            sizeof(double) * stage_n,                                     // FP64 staging
+                            sizeof(d.table), sizeof(unsigned),                            // table, error flag
+                            sizeof(double) * DIAG_VALUES * (h->nblocks + FINALIZE_BLOCKS),  // partials
+                            sizeof(unsigned), sizeof(double) * DIAG_VALUES};              // flag, diagnostics
+    size_t total = 0;
+    for (size_t b : sizes) total += (b + 255) / 256 * 256;
+    char *base = nullptr;
+    TRY(dev_alloc(h, &base, total, "handle buffers"));
+    size_t off = 0;
+    auto take = [&](int i) {
+      void *p = base + off;
+      off += (sizes[i] + 255) / 256 * 256;
+      return p;
+    };
+    d.f = take(0);
+    d.cls = static_cast<uint8_t *>(take(1));
+    d.rho = take(2);
+    for (int k = 0; k < 3; k++) {
+      void *p = take(3 + k);
+      if (k < d.dim) d.u[k] = p;
+    }
+    if (d.dim == 2) d.u[2] = d.u[1];  // never written for D2Q9; keeps pointers valid
+    h->fetch_stage = static_cast<double *>(take(6));
+    h->fetch_stage_n = stage_n;
+    d.table_dev = static_cast<uint16_t *>(take(7));
+    d.error_flag = static_cast<unsigned *>(take(8));
+    d.partials = static_cast<double *>(take(9));
+    d.flag = static_cast<unsigned *>(take(10));
+    h->diag_out = static_cast<double *>(take(11));
+  }
+  TRYCUDA(cudaMemsetAsync(d.error_flag, 0, sizeof(unsigned), h->stream), "clear error flag");
+  TRYCUDA(cudaMemsetAsync(d.flag, 0, sizeof(unsigned), h->stream), "clear flag");
+
+  // The node classes are checked and packed on the host's cores while this
+  // thread uploads rho and u (DMA): the two take similar times and do not
+  // depend on each other.  The packing thread
+  // reads only cfg and dom; an invalid domain is reported once it has
+  // joined (uploads of absent arrays fill zeros, so nothing reads past what
+  // the caller passed).
+  HostClasses hc;
+  lbmc_status cls_status = LBMC_OK;
+  std::string cls_error;
+  std::thread cls_thread([&] {
+    cls_status = build_classes(cfg, dom, n, hc, true);
+    if (cls_status != LBMC_OK) cls_error = lbmc_last_error();
+  });
+  struct Joiner {
+    std::thread &t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } joiner{cls_thread};
 
   // rho - 1 and u: prescribed input (macro BC) and stored output.
-  TRY(dev_alloc(h, &d.rho, (size_t)n * cs, "rho"));
   TRY(upload_compute(h, d.rho, dom->rho, n, -1.0, 0.0));
-  for (int k = 0; k < 3; k++) {
-    if (k < d.dim) {
-      TRY(dev_alloc(h, &d.u[k], (size_t)n * cs, "u"));
-      TRY(upload_compute(h, d.u[k], dom->u[k], n, 0.0, 0.0));
-    }
-  }
-  if (d.dim == 2) d.u[2] = d.u[1];  // never written for D2Q9; keeps pointers valid
+  for (int k = 0; k < d.dim; k++) TRY(upload_compute(h, d.u[k], dom->u[k], n, 0.0, 0.0));
 
   cls_thread.join();
   if (cls_status != LBMC_OK) {
@@ -570,6 +713,7 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
   memcpy(d.table, hc.table, sizeof(d.table));
   d.blend = hc.any_partial ? 1 : 0;
   TRYCUDA(cudaMemcpy(d.cls, hc.cls.data(), n, cudaMemcpyHostToDevice), "upload classes");
+  TRYCUDA(cudaMemcpy(d.table_dev, d.table, sizeof(d.table), cudaMemcpyHostToDevice), "upload class table");
 
   if (hc.any_partial) {
     TRY(dev_alloc(h, &d.B, (size_t)n * cs, "porosity"));
@@ -612,37 +756,6 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
     TRYCUDA(cudaMemcpy(d.sf_index, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload sf");
     TRYCUDA(cudaMemset(d.sf_buf, 0, (size_t)cs * q * d.n_sf), "clear sf");
   }
-
-  TRY(dev_alloc(h, &d.table_dev, sizeof(d.table), "class table"));
-  TRYCUDA(cudaMemcpy(d.table_dev, d.table, sizeof(d.table), cudaMemcpyHostToDevice), "upload class table");
-  TRY(dev_alloc(h, &d.error_flag, sizeof(unsigned), "error flag"));
-  TRYCUDA(cudaMemset(d.error_flag, 0, sizeof(unsigned)), "clear error flag");
-  {
-    int khz = 0;
-    cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, cfg->device);
-    // Every device-side wait gives up after about two seconds.
-    d.timeout_cycles = (long long)(khz > 0 ? khz : 2000000) * 1000LL * 2;
-  }
-  d.aa = cfg->streaming == LBMC_STREAM_AA ? 1 : 0;
-  // The tiled AA layout needs whole 64-node tiles along x (one direct-kernel
-  // block each) and element indices over all Q arrays below 2^32 (its row
-  // and x offsets are 32-bit); other domains keep the plain AA layout.
-  d.tiled = d.aa && d.L[0] % lbmc::TILE == 0 && (long long)q * n < (1ll << 32) ? 1 : 0;
-  d.pipeline = cfg->kernel == LBMC_KERNEL_PIPELINED ? 2 : 0;
-  TRYCUDA(h->ops->plan(d), "kernel planning");
-  if (cfg->kernel == LBMC_KERNEL_PIPELINED && !d.use_pipeline) {
-    release(h);
-    return fail(LBMC_ERR_UNSUPPORTED,
-                "the bulk-copy pipeline needs Lx * element size to be a multiple of 16 bytes "
-                "and two stages of Q rows to fit in shared memory");
-  }
-  h->nblocks = d.nblocks;
-  // Per-block partials of the step, then the finalize blocks' sums.
-  TRY(dev_alloc(h, &d.partials, sizeof(double) * DIAG_VALUES * (h->nblocks + FINALIZE_BLOCKS),
-                "diagnostic partials"));
-  TRY(dev_alloc(h, &d.flag, sizeof(unsigned), "diagnostic flag"));
-  TRY(dev_alloc(h, &h->diag_out, sizeof(double) * DIAG_VALUES, "diagnostics"));
-  TRYCUDA(cudaMemset(d.flag, 0, sizeof(unsigned)), "clear flag");
 
   // Initial populations (Init: model_builder.cu:227-248 for Init 0).
   if (cfg->init_type == LBMC_INIT_STATIC) {
