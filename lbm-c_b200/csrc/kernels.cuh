@@ -219,11 +219,36 @@ __device__ __forceinline__ void store_node_sr(const float (&out)[Q], float scale
     constexpr int k = decltype(pc)::value;
     constexpr int i0 = 2 * k, i1 = 2 * k + 1;
     const unsigned r = k == 0 ? h : sr_word(h, k);
-    float hi = 0.0f;
-    if constexpr (i1 < Q) hi = out[i1] * scale;
-    const unsigned d = cvt_rs_f16x2(hi, out[i0] * scale, r);
+    // the pair's scale multiply as one packed FP32x2 multiply (same roundings)
+    float o1 = 0.0f;
+    if constexpr (i1 < Q) o1 = out[i1];
+    const float2 v = __fmul2_rn(make_float2(out[i0], o1), make_float2(scale, scale));
+    const unsigned d = cvt_rs_f16x2(v.y, v.x, r);
     put16(ptr(std::integral_constant<int, i0>{}), (unsigned short)(d & 0xffffu));
     if constexpr (i1 < Q) put16(ptr(std::integral_constant<int, i1>{}), (unsigned short)(d >> 16));
+  });
+}
+
+// Writes a node's Q post-collision values to FP16 storage rounded to
+// nearest, two per conversion: the scale multiply of a population pair is
+// one packed FP32x2 multiply (mul.rn.f32x2) and the pair converts with one
+// cvt.rn.f16x2.f32.  Every value is rounded exactly as the one-value path
+// rounds it (v * scale, then to nearest FP16); only the instruction count
+// differs.
+template <int Q, class Ptr>
+__device__ __forceinline__ void store_node_f16(const float (&out)[Q], float scale, Ptr &&ptr) {
+  unroll<(Q + 1) / 2>([&](auto pc) {
+    constexpr int k = decltype(pc)::value;
+    constexpr int i0 = 2 * k, i1 = 2 * k + 1;
+    auto put16 = [](auto *p, unsigned short v) { __stcs(reinterpret_cast<unsigned short *>(p), v); };
+    if constexpr (i1 < Q) {
+      const float2 v = __fmul2_rn(make_float2(out[i0], out[i1]), make_float2(scale, scale));
+      const __half2 h = __floats2half2_rn(v.x, v.y);
+      put16(ptr(std::integral_constant<int, i0>{}), __half_as_ushort(__low2half(h)));
+      put16(ptr(std::integral_constant<int, i1>{}), __half_as_ushort(__high2half(h)));
+    } else {
+      put16(ptr(std::integral_constant<int, i0>{}), __half_as_ushort(__float2half_rn(out[i0] * scale)));
+    }
   });
 }
 
@@ -1268,6 +1293,8 @@ __global__ void __launch_bounds__(DIRECT_BLOCK, (direct_min_blocks<S, COL>()))
         if constexpr (stochastic_storage<S>())
           store_node_sr<Q, true>(out, scale, (unsigned)n ^ a.sr_seed,
                                  [&](auto ic) { return write_at(f, sw, tw, n, ic); });
+        else if constexpr (std::is_same<S, __half>::value)
+          store_node_f16<Q>(out, scale, [&](auto ic) { return write_at(f, sw, tw, n, ic); });
         else
           unroll<Q>([&](auto ic) { store_dev(write_at(f, sw, tw, n, ic), out[decltype(ic)::value], scale); });
       };
