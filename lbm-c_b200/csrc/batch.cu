@@ -1,7 +1,9 @@
 // Batched persistent step for many independent small D2Q9 domains
 // (lbmc_batch_*).  No counterpart in the reference, which runs one domain per
 // process; each domain here is stepped exactly as lbmc_iterate steps a single
-// domain (same shift layout, same collide_fluid), so parity is inherited.
+// domain (the shift layout with FP32 storage and the AA pattern of
+// LBMC_STREAM_AA with 2-byte storage, the same collide_fluid), so parity is
+// inherited.
 //
 // Execution model.  Domains whose populations fit in a block's shared
 // memory are stepped by one persistent kernel: blocks take whole domains
@@ -91,13 +93,74 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// One D2Q9 node in the AA pattern (one array per population, in place;
+// 2-byte storage, see batch_aa below):
+// at an even step the node reads population i from its own slot of array i
+// and writes out[i] to its own slot of array opp(i); at an odd step it reads
+// population i from array opp(i) at x - e_i and writes out[i] to array i at
+// x + e_i (periodic wrap).  A node writes exactly the slots it read, so the
+// update is race-free in place, and the state after every step equals the
+// shift layout's up to where the values sit (the single-domain engine's
+// LBMC_STREAM_AA maps).  Collide, write back; returns u = j/rho + F/(2 rho)
+// in `u` (the stored velocity of LBM-C/collision.cu:77).
+template <class S, bool BLEND, bool ODD>
+__device__ __forceinline__ void batch_node_aa(S *pop, long long pitch, int k, int x, int y, int lx, int ly,
+                                              int cls, const StepArgs<float> &a, float &ux, float &uy) {
+  using L = D2Q9;
+  int xs[3] = {x, x, x}, ys[3] = {y, y, y};
+  if constexpr (ODD) {
+    xs[1] = wrap_sub(x, 1, lx);
+    xs[2] = wrap_add(x, 1, lx);
+    ys[1] = wrap_sub(y, 1, ly);
+    ys[2] = wrap_add(y, 1, ly);
+  }
+  Node<L, float> nd;
+  unroll<9>([&](auto ic) {
+    constexpr int i = decltype(ic)::value;
+    if constexpr (ODD) {
+      const int slot = xs[sel(L::e(0, i))] + lx * ys[sel(L::e(1, i))];
+      nd.g[i] = load_dev(pop + L::opp(i) * pitch + slot, a.inv_scale);
+    } else {
+      nd.g[i] = load_dev(pop + i * pitch + k, a.inv_scale);
+    }
+  });
+  float out[9];
+  if (cls == CLASS_SOLID) {
+    collide_solid(nd, out);
+  } else {
+    moments(nd);
+    // a.B is this domain's porosity array; only partial nodes read it.
+    collide_fluid<L, float, COL_BGK, true, BLEND, true>(nd, a, k, cls == 2 ? ENTRY_PARTIAL : 0u, out);
+  }
+  if constexpr (ODD) {
+    // The store slots equal the load slots; recomputing them from the six
+    // coordinates is cheaper than keeping nine addresses live across the
+    // collision (the empty asm hides the equality from the compiler).
+    int xw[3] = {xs[0], xs[1], xs[2]}, yw[3] = {ys[0], ys[1], ys[2]};
+    asm("" : "+r"(xw[0]), "+r"(xw[1]), "+r"(xw[2]), "+r"(yw[0]), "+r"(yw[1]), "+r"(yw[2]));
+    unroll<9>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      constexpr int o = L::opp(i);
+      const int slot = xw[sel(L::e(0, o))] + lx * yw[sel(L::e(1, o))];
+      store_smem(pop + i * pitch + slot, out[i], a.scale);
+    });
+  } else {
+    unroll<9>([&](auto ic) {
+      constexpr int i = decltype(ic)::value;
+      store_smem(pop + L::opp(i) * pitch + k, out[i], a.scale);
+    });
+  }
+  ux = nd.u[0];
+  uy = nd.u[1];
+}
+
 // One D2Q9 node: load its 9 shift slots from `pop` (pitch elements apart),
 // collide, write back; returns u = j/rho + F/(2 rho) in `u` (the stored
 // velocity of LBM-C/collision.cu:77).
 template <class S, bool BLEND>
-__device__ __forceinline__ void batch_node(S *pop, long long pitch, int k, int x, int y, int lx, int ly,
-                                           int sx, int sy, int cls, const StepArgs<float> &a,
-                                           float &ux, float &uy) {
+__device__ __forceinline__ void batch_node_shift(S *pop, long long pitch, int k, int x, int y, int lx, int ly,
+                                                 int sx, int sy, int cls, const StepArgs<float> &a,
+                                                 float &ux, float &uy) {
   using L = D2Q9;
   const int xs[3] = {x, wrap_sub(x, sx, lx), wrap_add(x, sx, lx)};
   const int ys[3] = {y, wrap_sub(y, sy, ly), wrap_add(y, sy, ly)};
@@ -127,6 +190,29 @@ __device__ __forceinline__ void batch_node(S *pop, long long pitch, int k, int x
   });
   ux = nd.u[0];
   uy = nd.u[1];
+}
+
+// The layout of the batched domains, per storage format.  Measured on the
+// 4096-domain sweep (first 20,000 steps, one B200): 2-byte storage 80.1
+// GLUPS in the shift layout, 84.9 in the AA pattern; FP32 55.4 shift, 51.1-53.9
+// AA (its wide kernel, which FP16 does not use by default, holds both AA
+// maps and spills or loses occupancy at its register cap).
+template <class S>
+__host__ __device__ constexpr bool batch_aa() {
+  return sizeof(S) == 2;
+}
+
+// The step of node k at step t: shift t mod (lx, ly) or AA parity t & 1.
+template <class S, bool BLEND>
+__device__ __forceinline__ void batch_node(S *pop, long long pitch, int k, int x, int y, int lx, int ly,
+                                           int sx, int sy, bool odd, int cls, const StepArgs<float> &a,
+                                           float &ux, float &uy) {
+  if constexpr (batch_aa<S>()) {
+    if (odd) batch_node_aa<S, BLEND, true>(pop, pitch, k, x, y, lx, ly, cls, a, ux, uy);
+    else batch_node_aa<S, BLEND, false>(pop, pitch, k, x, y, lx, ly, cls, a, ux, uy);
+  } else {
+    batch_node_shift<S, BLEND>(pop, pitch, k, x, y, lx, ly, sx, sy, cls, a, ux, uy);
+  }
 }
 
 // The convergence measure keeps a non-finite velocity visible: fmaxf
@@ -212,7 +298,8 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
     long long t = st.t;
     int stop = 0;
     for (int s = 0; s < A.steps && !stop; s++, t++) {
-      const int sx = (int)(t % D.lx), sy = (int)(t % D.ly);
+      const int sx = batch_aa<S>() ? 0 : (int)(t % D.lx), sy = batch_aa<S>() ? 0 : (int)(t % D.ly);
+      const bool odd = t & 1;
       // Every C steps: du = max |u(t) - u(t - C)|, then u(t) is kept for the
       // next check.  Reduced-precision dynamics that settle into a fixed point
       // or a cycle whose period divides C give exactly zero.
@@ -225,7 +312,7 @@ __global__ void __launch_bounds__(1024) batch_kernel(const BatchArgs A) {
       for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int c = cls[k];
         float ux, uy;
-        batch_node<S, BLEND>(pop, pitch, k, x, y, D.lx, D.ly, sx, sy, c, a, ux, uy);
+        batch_node<S, BLEND>(pop, pitch, k, x, y, D.lx, D.ly, sx, sy, odd, c, a, ux, uy);
         if (test) dmax = nan_max(dmax, node_delta(ux, uy, up[k]));
         if (save) up[k] = make_float2(ux, uy);
         x += step_x;
@@ -289,20 +376,21 @@ struct RowSegment {
 };
 // What the next step of a listed domain needs, prepared once per domain and
 // step (by the host when the list is built, then by the finish kernel), so
-// that no warp divides the 64-bit step counter: the shift t mod (lx, ly) and
-// the flags below.
+// that no warp divides the 64-bit step counter: the shift t mod (lx, ly),
+// the parity of t (AA) and the flags below.
 struct WideStep {
   int sx, sy;
   int flags;
 };
-constexpr int WIDE_RUNNING = 1, WIDE_SAVE = 2, WIDE_TEST = 4;
+constexpr int WIDE_RUNNING = 1, WIDE_SAVE = 2, WIDE_TEST = 4, WIDE_ODD = 8;
 
 __host__ __device__ inline WideStep wide_step(long long t, int lx, int ly, int check, bool running) {
   WideStep w;
   w.sx = (int)(t % lx);
   w.sy = (int)(t % ly);
   const bool save = (t % check) == 0;
-  w.flags = (running ? WIDE_RUNNING : 0) | (save ? WIDE_SAVE : 0) | (save && t >= check ? WIDE_TEST : 0);
+  w.flags = (running ? WIDE_RUNNING : 0) | (save ? WIDE_SAVE : 0) | (save && t >= check ? WIDE_TEST : 0) |
+            ((t & 1) ? WIDE_ODD : 0);
   return w;
 }
 
@@ -312,8 +400,16 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
+// Resident blocks of the wide kernel per SM: the register cap of 20 blocks
+// (48 registers) holds the shift step; the AA step (both maps in one kernel)
+// spills 28-76 bytes there and 0-24 at 18 blocks (56 registers).
+template <class S>
+constexpr int wide_min_blocks() {
+  return batch_aa<S>() ? 18 : 20;
+}
+
 template <class S, bool BLEND>
-__global__ void __launch_bounds__(WIDE_THREADS, 20)
+__global__ void __launch_bounds__(WIDE_THREADS, (wide_min_blocks<S>()))
     batch_wide_kernel(const BatchArgs A, const RowSegment *segs, int nsegs, const WideStep *steps, int *acc) {
   const int si = blockIdx.x * WIDE_WARPS + (int)(threadIdx.x >> 5);
   if (si >= nsegs) return;  // whole warps
@@ -336,6 +432,7 @@ __global__ void __launch_bounds__(WIDE_THREADS, 20)
   a.inv_scale = A.inv_scale;
   const BatchDomainDev D = A.dom[G.domain];
   const int sx = W.sx, sy = W.sy;
+  const bool odd = W.flags & WIDE_ODD;
   const bool save = W.flags & WIDE_SAVE;
   const bool test = W.flags & WIDE_TEST;
   a.B = A.B + D.node_off;
@@ -351,7 +448,7 @@ __global__ void __launch_bounds__(WIDE_THREADS, 20)
     if (y >= D.ly) break;  // past the domain's last node
     const int k = x + y * D.lx;
     float ux, uy;
-    batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, y, D.lx, D.ly, sx, sy, A.cls[D.node_off + k], a,
+    batch_node<S, BLEND>(pool + D.pop_off, D.pitch, k, x, y, D.lx, D.ly, sx, sy, odd, A.cls[D.node_off + k], a,
                          ux, uy);
     if (test) dmax = nan_max(dmax, node_delta(ux, uy, up[k]));
     if (save) up[k] = make_float2(ux, uy);
@@ -898,13 +995,19 @@ __global__ void batch_fetch_kernel(const S *pop, long long pitch, int lx, int ly
   if (k >= lx * ly) return;
   using L = D2Q9;
   const int x = k % lx, y = k / lx;
-  const int sx = (int)(t % lx), sy = (int)(t % ly);
-  const int xs[3] = {x, wrap_sub(x, sx, lx), wrap_add(x, sx, lx)};
-  const int ys[3] = {y, wrap_sub(y, sy, ly), wrap_add(y, sy, ly)};
+  // Shift layout: population i of node x in array i at (x - t e_i) mod L.
+  // AA pattern: after an even number of steps in array i at x; after an odd
+  // number in array opp(i) at x - e_i (the next, odd step's read map).
+  const bool odd = batch_aa<S>() && (t & 1);
+  const int sx = batch_aa<S>() ? (odd ? 1 : 0) : (int)(t % lx);
+  const int sy = batch_aa<S>() ? (odd ? 1 : 0) : (int)(t % ly);
+  const int xs[3] = {x, wrap_sub(x, sx % lx, lx), wrap_add(x, sx % lx, lx)};
+  const int ys[3] = {y, wrap_sub(y, sy % ly, ly), wrap_add(y, sy % ly, ly)};
   double r = 0, jx = 0, jy = 0;
   for (int i = 0; i < 9; i++) {
     const int slot = xs[sel(L::e(0, i))] + lx * ys[sel(L::e(1, i))];
-    const double v = weight<L>(i) + (double)load_dev(pop + i * pitch + slot, inv_scale);
+    const int arr = odd ? L::opp(i) : i;
+    const double v = weight<L>(i) + (double)load_dev(pop + arr * pitch + slot, inv_scale);
     if (f) f[(long long)i * lx * ly + k] = v;
     r += v;
     jx += L::e(0, i) * v;
