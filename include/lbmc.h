@@ -191,7 +191,11 @@ typedef struct lbmc_diag {
 lbmc_status lbmc_config_default(lbmc_config *cfg, int lattice);
 
 /* Replaces setup() (LBM-C/index.cu:157-186) and ModelBuilder
- * (LBM-C/model_builder.cu:257-278). */
+ * (LBM-C/model_builder.cu:257-278).  Rejects what lbmc_validate rejects,
+ * with the same status and message: configuration errors before any device
+ * work, per-node input errors (codes, porosity, fields a code needs) once
+ * the host's check of the arrays, which runs while rho and u upload, ends;
+ * nothing is left allocated on failure. */
 lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
                       lbmc_handle **out);
 
