@@ -7,9 +7,10 @@
 
 namespace lbmc {
 
-// Shared memory of the pipelined kernel's stages, per block: with
-// PIPE_MIN_BLOCKS resident blocks, 4 x 48 KB of the SM's 228 KB.
-constexpr long long PIPE_STAGE_BUDGET = 48 * 1024;
+// Shared memory of the pipelined kernel's stages, per block (at least two
+// stages of Q rows): with FP32 rows of 256 nodes, two stages, seven blocks
+// per SM.
+constexpr long long PIPE_STAGE_BUDGET = 32 * 1024;
 
 template <class L, class S>
 struct Launchers {
@@ -82,10 +83,10 @@ struct Launchers {
     if (st > PIPE_MAX_STAGES) st = PIPE_MAX_STAGES;
     return (int)st;
   }
-  // One producer warp plus up to STEP_BLOCK / 32 consumer warps.
+  // One producer warp plus up to pipe_consumers<S>() / 32 consumer warps.
   static int pipe_threads(const DeviceState &d) {
     int bx = (d.L[0] + 31) / 32 * 32;
-    return 32 + (bx < STEP_BLOCK ? bx : STEP_BLOCK);
+    return 32 + (bx < pipe_consumers<S>() ? bx : pipe_consumers<S>());
   }
 
   template <int COL, bool FORCE, bool BLEND, bool DIAG>

@@ -1466,14 +1466,20 @@ __device__ __forceinline__ void issue_row_store(S *f, long long pitch, long long
 }
 
 constexpr int PIPE_MAX_STAGES = 8;
-// Four blocks per SM (56 registers a thread, 48 KB of stages a block): FP32
-// 28.7 -> 41.0 GLUPS, FP16 26.4 -> 37.6 on the porous 256^3 step against two
-// blocks with 90-96 registers and 96 KB of stages.
-constexpr int PIPE_MIN_BLOCKS = 4;
+// Launch shape: consumer threads per block and the register cap (resident
+// blocks per SM), with 32 KB of stages per block.  Many small blocks, each
+// consumer stepping several nodes of a row, beat few large ones: on the
+// porous 256^3 step, FP32 28.7 GLUPS (2 blocks of 256 consumers, 96 KB of
+// stages) -> 41.0 (4 blocks, 48 KB) -> 46.6 (64 consumers, 7 blocks by
+// shared memory); FP16 26.4 -> 37.6 -> 45.7 with 128 consumers (64: 44.2).
+// Every shape caps registers at 56 a thread; FP64 keeps its register pairs.
+template <class S>
+constexpr int pipe_consumers() {
+  return sizeof(S) == 2 ? 128 : 64;
+}
 template <class S>
 constexpr int pipe_min_blocks() {
-  // FP64 arithmetic needs register pairs: no cap beyond the block size's.
-  return std::is_same<S, double>::value ? 1 : PIPE_MIN_BLOCKS;
+  return std::is_same<S, double>::value ? 1 : (65536 / 56) / (pipe_consumers<S>() + 32);
 }
 
 __device__ __forceinline__ void mbar_arrive(unsigned bar) {
@@ -1491,7 +1497,7 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar) {
 // bounded waits and returns.
 // Dynamic shared memory: [stages][Q][Lx] storage elements.
 template <class L, class S, int COL, bool FORCE, bool BLEND, bool DIAG>
-__global__ void __launch_bounds__(STEP_BLOCK + 32, (pipe_min_blocks<S>()))
+__global__ void __launch_bounds__(pipe_consumers<S>() + 32, (pipe_min_blocks<S>()))
     step_pipelined_kernel(const StepArgs<typename Storage<S>::C> a) {
   using C = typename Storage<S>::C;
   constexpr int Q = L::Q;

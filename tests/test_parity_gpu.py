@@ -271,13 +271,14 @@ def test_pipelined_and_direct_kernels_agree(lbmc, storage):
 
 @pytest.mark.parametrize("storage", ["f32", "f16"])
 def test_pipelined_kernel_reuses_its_stages(lbmc, storage):
-    """Many more grid rows (96 x 64 = 6144) than resident pipelined blocks
-    (four per SM) times their stages (at most eight), so every block walks
-    its rows through the stages more than once: each stage is stored and
-    reloaded, and the mbarrier phases wrap.
+    """More grid rows (64 x 80 = 5120) than the resident pipelined blocks
+    (seven per SM with rows of 256 nodes) times their stages (two FP32 or
+    four FP16 rows of populations), so every block walks its rows through
+    the stages more than once: each stage is stored and reloaded, and the
+    mbarrier phases wrap.
     The result must equal the direct kernel's bit for bit, after odd and even
     step counts."""
-    case = make_case("d3q15", (32, 96, 64), 2, True, solids=0.1, micro="zh", macro="random", seed=21)
+    case = make_case("d3q15", (256, 64, 80), 2, True, solids=0.1, micro="zh", macro="random", seed=21)
     for steps in (7, 12):
         a = run_engine(lbmc, case, steps, storage, kernel=lbmc.KERNEL_DIRECT)
         b = run_engine(lbmc, case, steps, storage, kernel=lbmc.KERNEL_PIPELINED)
