@@ -251,13 +251,15 @@ def test_init_large_is_exact_and_repeatable(lbmc, length, init):
             np.testing.assert_allclose(eng.f(), expect, rtol=0, atol=1e-15)
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f16sr", "bf16", "f64"])
 def test_pipelined_and_direct_kernels_agree(lbmc, storage):
     """The two step kernels run the same collision code: identical bits with
-    FP32 and FP16 storage.  In FP64 the compiler may fuse a multiply and an
-    add into one FMA in one kernel and not in the other (the two inline the
-    collision into different surroundings), so they agree to a few units in
-    the last place (4e-16 relative to the largest value after 25 steps)."""
+    FP32, FP16 (also with stochastic rounding, whose random bits depend on
+    node, step and population only) and BF16 storage.  In FP64 the compiler
+    may fuse a multiply and an add into one FMA in one kernel and not in the
+    other (the two inline the collision into different surroundings), so
+    they agree to a few units in the last place (4e-16 relative to the
+    largest value after 25 steps)."""
     case = make_case("d3q15", (32, 20, 12), 3, True, solids=0.1, partial=0.1, micro="zh",
                      macro="random", seed=12)
     a = run_engine(lbmc, case, 25, storage, kernel=lbmc.KERNEL_DIRECT)
@@ -269,7 +271,7 @@ def test_pipelined_and_direct_kernels_agree(lbmc, storage):
             np.testing.assert_array_equal(x, y)
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f16sr", "bf16"])
 def test_pipelined_kernel_reuses_its_stages(lbmc, storage):
     """More grid rows (64 x 80 = 5120) than the resident pipelined blocks
     (seven per SM with rows of 256 nodes) times their stages (two FP32 or
