@@ -637,7 +637,7 @@ extern "C" lbmc_status lbmc_init(const lbmc_config *cfg, const lbmc_domain *dom,
 
   // The buffers every handle holds come from one cudaMalloc, carved at
   // 256-byte boundaries: each cudaMalloc of a large buffer measured 1-5 ms
-  // (page mapping in the driver), about as long as the upload of a field.
+  // inside lbmc_init, about as long as the upload of a field.
   {
     // Populations: Q arrays, each padded to a 256-byte boundary.
     const long long align = 256 / ss;
